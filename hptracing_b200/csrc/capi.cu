@@ -1,0 +1,753 @@
+// C ABI: device-resident scenes, render, per-stage entry points, stream
+// compaction, batching. (Host-only producers live in capi_host.cpp.)
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/hpt.h"
+#include "engine.h"
+#include "scene_pack.h"
+#include "shading.cuh"
+#include "traverse.cuh"
+
+using namespace hpt;
+
+struct hpt_scene {
+  SceneHandle h;
+};
+
+namespace hpt {
+
+namespace {
+
+template <typename T>
+hpt_status dev_upload(SceneDev& s, const T* host, size_t count, const T** out) {
+  *out = nullptr;
+  if (count == 0) return HPT_OK;
+  void* p = nullptr;
+  HPT_CUDA(cudaMalloc(&p, count * sizeof(T)));
+  s.allocations.push_back(p);
+  s.bytes += (int64_t)(count * sizeof(T));
+  HPT_CUDA(cudaMemcpy(p, host, count * sizeof(T), cudaMemcpyHostToDevice));
+  *out = static_cast<const T*>(p);
+  return HPT_OK;
+}
+
+// Device buffer for stage entry points: upload (optional) and download.
+struct DBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DBuf() {
+    if (p) cudaFree(p);
+  }
+  hpt_status alloc(size_t b) {
+    bytes = b;
+    if (b == 0) return HPT_OK;
+    HPT_CUDA(cudaMalloc(&p, b));
+    return HPT_OK;
+  }
+  hpt_status up(const void* host, size_t b) {
+    hpt_status s = alloc(b);
+    if (s != HPT_OK || b == 0) return s;
+    HPT_CUDA(cudaMemcpy(p, host, b, cudaMemcpyHostToDevice));
+    return HPT_OK;
+  }
+  hpt_status down(void* host) const {
+    if (!host || bytes == 0) return HPT_OK;
+    HPT_CUDA(cudaMemcpy(host, p, bytes, cudaMemcpyDeviceToHost));
+    return HPT_OK;
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Stage kernels (one thread per element).
+// ---------------------------------------------------------------------------
+__global__ void k_stage_intersect(const DevScene* s, int n, const float* o, const float* d,
+                                  int32_t* tri, float* t, float* u, float* v, uint32_t* err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  TravState st;
+  trav_init(*s, Ray{mk(o[3 * i], o[3 * i + 1], o[3 * i + 2]), mk(d[3 * i], d[3 * i + 1], d[3 * i + 2])},
+            st);
+  TravCount cnt;
+  while (!trav_leaf(*s, st, nullptr, 0, err, cnt)) {
+  }
+  tri[i] = st.best.tri;
+  t[i] = st.best.rec >= 0 ? st.best.t : 0.f;
+  u[i] = st.best.rec >= 0 ? st.best.u : 0.f;
+  v[i] = st.best.rec >= 0 ? st.best.v : 0.f;
+}
+
+__global__ void k_stage_shade(const DevScene* s, int n, const float* o, const float* d,
+                              const float* strength, const int32_t* tri, const float* t,
+                              uint64_t* seeds, int disable_diffuse, float* contrib,
+                              int32_t* branch, float* hit_p, float* normal, float* strength_out,
+                              float* param) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t seed = seeds[i];
+  const Ray r{mk(o[3 * i], o[3 * i + 1], o[3 * i + 2]), mk(d[3 * i], d[3 * i + 1], d[3 * i + 2])};
+  const ShadeOut so = shade_hit(*s, r, mk(strength[3 * i], strength[3 * i + 1], strength[3 * i + 2]),
+                                tri[i], t[i], disable_diffuse, seed);
+  seeds[i] = seed;
+  contrib[3 * i] = so.contrib.x; contrib[3 * i + 1] = so.contrib.y; contrib[3 * i + 2] = so.contrib.z;
+  hit_p[3 * i] = so.hit_p.x; hit_p[3 * i + 1] = so.hit_p.y; hit_p[3 * i + 2] = so.hit_p.z;
+  normal[3 * i] = so.normal.x; normal[3 * i + 1] = so.normal.y; normal[3 * i + 2] = so.normal.z;
+  strength_out[3 * i] = so.strength.x;
+  strength_out[3 * i + 1] = so.strength.y;
+  strength_out[3 * i + 2] = so.strength.z;
+  param[i] = so.param;
+  branch[i] = so.branch;
+}
+
+__global__ void k_stage_next(const DevScene* s, int n, const int32_t* branch, const float* d,
+                             const float* hit_p, const float* normal, const float* strength,
+                             const float* param, uint64_t* seeds, float* o_out, float* d_out,
+                             float* s_out, int32_t* alive) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t seed = seeds[i];
+  const NextOut no = next_direction(*s, branch[i], mk(d[3 * i], d[3 * i + 1], d[3 * i + 2]),
+                                    mk(hit_p[3 * i], hit_p[3 * i + 1], hit_p[3 * i + 2]),
+                                    mk(normal[3 * i], normal[3 * i + 1], normal[3 * i + 2]),
+                                    mk(strength[3 * i], strength[3 * i + 1], strength[3 * i + 2]),
+                                    param[i], seed);
+  seeds[i] = seed;
+  o_out[3 * i] = no.o.x; o_out[3 * i + 1] = no.o.y; o_out[3 * i + 2] = no.o.z;
+  d_out[3 * i] = no.d.x; d_out[3 * i + 1] = no.d.y; d_out[3 * i + 2] = no.d.z;
+  s_out[3 * i] = no.strength.x; s_out[3 * i + 1] = no.strength.y; s_out[3 * i + 2] = no.strength.z;
+  alive[i] = no.alive ? 1 : 0;
+}
+
+__global__ void k_stage_raygen(hpt_camera cam, int nx, int ny, int pano, int x_shift, float* o,
+                               float* d) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= nx || y >= ny) return;
+  const f3 dir = pano ? pano_dir(x, y, x_shift, ny)
+                      : pinhole_dir(cam.top_dir, cam.right_dir, cam.width, cam.height, x, y, nx, ny);
+  const int64_t idx = (int64_t)nx * y + x;
+  o[3 * idx] = cam.view_p[0]; o[3 * idx + 1] = cam.view_p[1]; o[3 * idx + 2] = cam.view_p[2];
+  d[3 * idx] = dir.x; d[3 * idx + 1] = dir.y; d[3 * idx + 2] = dir.z;
+}
+
+__device__ __forceinline__ uint8_t unorm8(float x) {
+  const float v = __fmul_rn(x, 255.0f);
+  if (!(v >= 0.f)) return 0;
+  if (v >= 255.f) return 255;
+  return (uint8_t)__float2int_rn(v);
+}
+
+__global__ void k_stage_resolve(const float* accum, int W, int H, int ssx, int ssy, int spp,
+                                float brightness, uint8_t* rgba) {
+  const int gx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (gx >= W || gy >= H) return;
+  float p[3] = {0.f, 0.f, 0.f};
+  for (int i = 0; i < ssx; ++i)
+    for (int j = 0; j < ssy; ++j) {
+      const int64_t idx = (int64_t)(gy * ssy + j) * W * ssx + gx * ssx + i;
+      for (int c = 0; c < 3; ++c) p[c] = __fadd_rn(p[c], accum[3 * idx + c]);
+    }
+  uint8_t* out = rgba + 4 * ((int64_t)gy * W + gx);
+  for (int c = 0; c < 3; ++c) {
+    float x = __fmul_rn(__fdiv_rn(__fdiv_rn(p[c], (float)(ssx * ssy)), (float)spp), brightness);
+    out[c] = unorm8(__fsub_rn(1.f, expf(-x)));
+  }
+  out[3] = 0;
+}
+
+// --- Stream compaction: warp ballot + block scan, three passes. ---------
+constexpr int kCompactThreads = 256;
+constexpr int kCompactItems = 8;
+constexpr int kCompactTile = kCompactThreads * kCompactItems;
+
+__device__ __forceinline__ unsigned lane_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__global__ void k_compact_count(const uint32_t* flags, int n, int* block_counts) {
+  __shared__ int warp_sum[kCompactThreads / 32];
+  const int64_t tile = (int64_t)blockIdx.x * kCompactTile;
+  int cnt = 0;
+  for (int k = 0; k < kCompactItems; ++k) {
+    const int64_t i = tile + (int64_t)k * kCompactThreads + threadIdx.x;
+    const bool f = i < n && flags[i] != 0;
+    cnt += __popc(__ballot_sync(0xFFFFFFFFu, f));
+  }
+  if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int w = 0; w < kCompactThreads / 32; ++w) s += warp_sum[w];
+    block_counts[blockIdx.x] = s;
+  }
+}
+
+// Exclusive scan of the block counts in place (one block, chunked).
+__global__ void k_compact_scan(int* counts, int nb, int* total) {
+  __shared__ int buf[1024];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nb; base += 1024) {
+    const int i = base + threadIdx.x;
+    const int v = i < nb ? counts[i] : 0;
+    buf[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+      const int add = threadIdx.x >= off ? buf[threadIdx.x - off] : 0;
+      __syncthreads();
+      buf[threadIdx.x] += add;
+      __syncthreads();
+    }
+    if (i < nb) counts[i] = carry + buf[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry += buf[1023];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void k_compact_scatter(const uint32_t* flags, int n, const int* block_offsets,
+                                  int* out) {
+  __shared__ int warp_base[kCompactThreads / 32];
+  __shared__ int running;
+  const int64_t tile = (int64_t)blockIdx.x * kCompactTile;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) running = block_offsets[blockIdx.x];
+  __syncthreads();
+  for (int k = 0; k < kCompactItems; ++k) {
+    const int64_t i = tile + (int64_t)k * kCompactThreads + threadIdx.x;
+    const bool f = i < n && flags[i] != 0;
+    const unsigned m = __ballot_sync(0xFFFFFFFFu, f);
+    if (lane == 0) warp_base[warp] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int s = running;
+      for (int w = 0; w < kCompactThreads / 32; ++w) {
+        const int c = warp_base[w];
+        warp_base[w] = s;
+        s += c;
+      }
+      running = s;
+    }
+    __syncthreads();
+    if (f) out[warp_base[warp] + __popc(m & lane_lt())] = (int)i;
+    __syncthreads();
+  }
+}
+
+inline int blocks_for(int64_t n, int bs) { return (int)((n + bs - 1) / bs); }
+
+hpt_status check_scene_desc(const hpt_scene_desc& d) {
+  if (d.num_points < 0 || d.num_triangles <= 0 || d.num_nodes <= 0 || d.num_leaf_data < 0 ||
+      d.num_materials <= 0 || d.num_lights < 0 || d.num_textures < 0 || d.num_normals < 0 ||
+      d.num_texcoords < 0)
+    return fail(HPT_ERR_INVALID_ARGUMENT, "scene: negative or empty counts");
+  if (!d.points || !d.triangles || !d.nodes || !d.materials || (d.num_leaf_data && !d.leaf_data))
+    return fail(HPT_ERR_INVALID_ARGUMENT, "scene: missing buffers");
+  if (d.num_normals != 0 && d.num_normals != d.num_points)
+    return fail(HPT_ERR_INVALID_SCENE,
+                "scene: %d normals for %d vertices (normals are indexed by vertex id)",
+                d.num_normals, d.num_points);
+  if (d.num_texcoords != 0 && d.num_texcoords != d.num_points)
+    return fail(HPT_ERR_INVALID_SCENE, "scene: %d texcoords for %d vertices", d.num_texcoords,
+                d.num_points);
+  const F4* pts = reinterpret_cast<const F4*>(d.points);
+  for (int i = 0; i < d.num_points; ++i)
+    if (!std::isfinite(pts[i].x) || !std::isfinite(pts[i].y) || !std::isfinite(pts[i].z))
+      return fail(HPT_ERR_INVALID_SCENE, "scene: vertex %d is not finite", i);
+  const I4* tris = reinterpret_cast<const I4*>(d.triangles);
+  for (int i = 0; i < d.num_triangles; ++i) {
+    const I4& t = tris[i];
+    if (t.x < 0 || t.y < 0 || t.z < 0 || t.x >= d.num_points || t.y >= d.num_points ||
+        t.z >= d.num_points)
+      return fail(HPT_ERR_INVALID_SCENE, "scene: triangle %d vertex index out of range", i);
+    if (t.w < 0 || t.w >= d.num_materials)
+      return fail(HPT_ERR_INVALID_SCENE, "scene: triangle %d material %d out of range", i, t.w);
+  }
+  if (d.num_lights > 0 && !d.lights) return fail(HPT_ERR_INVALID_ARGUMENT, "scene: lights missing");
+  const I4* lights = reinterpret_cast<const I4*>(d.lights);
+  for (int i = 0; i < d.num_lights; ++i) {
+    const I4& t = lights[i];
+    if (t.x < 0 || t.y < 0 || t.z < 0 || t.x >= d.num_points || t.y >= d.num_points ||
+        t.z >= d.num_points)
+      return fail(HPT_ERR_INVALID_SCENE, "scene: light %d vertex index out of range", i);
+  }
+  for (int i = 0; i < d.num_materials; ++i) {
+    const hpt_ref_material& m = d.materials[i];
+    if (m.diffuse_texture_id >= d.num_textures || m.ambient_texture_id >= d.num_textures)
+      return fail(HPT_ERR_INVALID_SCENE, "scene: material %d references a missing texture", i);
+  }
+  if (d.num_textures > 0 && !d.texture_data)
+    return fail(HPT_ERR_INVALID_ARGUMENT, "scene: texture data missing");
+  if (d.texture_dims)
+    for (int i = 0; i < d.num_textures; ++i)
+      if (d.texture_dims[2 * i] <= 0 || d.texture_dims[2 * i + 1] <= 0)
+        return fail(HPT_ERR_INVALID_SCENE, "scene: texture %d has no texels", i);
+  return HPT_OK;
+}
+
+}  // namespace
+
+hpt_status upload_scene(const hpt_scene_desc& d, SceneDev& out) {
+  hpt_status s = check_scene_desc(d);
+  if (s != HPT_OK) return s;
+  PackedScene pk;
+  s = pack_scene(d, 8192, pk);
+  if (s != HPT_OK) return s;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(HPT_ERR_CUDA, "no CUDA device");
+  if (d.device < 0 || d.device >= ndev) return fail(HPT_ERR_INVALID_ARGUMENT, "bad device %d", d.device);
+  HPT_CUDA(cudaSetDevice(d.device));
+  out.device = d.device;
+  DevScene& ds = out.dev;
+  memset(&ds, 0, sizeof ds);
+  const DevNode* nodes;
+  const DevLeaf* leaves;
+  const DevTri* recs;
+  const int32_t* refs;
+  if ((s = dev_upload(out, pk.nodes.data(), pk.nodes.size(), &nodes)) != HPT_OK) return s;
+  if ((s = dev_upload(out, pk.leaves.data(), pk.leaves.size(), &leaves)) != HPT_OK) return s;
+  // At least one entry so the pointer is valid even for an empty tree.
+  if (pk.refs.empty()) pk.refs.push_back(0);
+  if ((s = dev_upload(out, pk.refs.data(), pk.refs.size(), &refs)) != HPT_OK) return s;
+  if ((s = dev_upload(out, pk.tris.data(), pk.tris.size(), &recs)) != HPT_OK) return s;
+  ds.nodes = nodes;
+  ds.leaves = leaves;
+  ds.leaf_refs = refs;
+  ds.tris = recs;
+  const float* f = nullptr;
+  if ((s = dev_upload(out, d.points, 4 * (size_t)d.num_points, &f)) != HPT_OK) return s;
+  ds.points = f;
+  if ((s = dev_upload(out, d.normals, 4 * (size_t)d.num_normals, &f)) != HPT_OK) return s;
+  ds.normals = f;
+  if ((s = dev_upload(out, d.texcoords, 2 * (size_t)d.num_texcoords, &f)) != HPT_OK) return s;
+  ds.texcoords = f;
+  const int32_t* ip = nullptr;
+  if ((s = dev_upload(out, d.triangles, 4 * (size_t)d.num_triangles, &ip)) != HPT_OK) return s;
+  ds.geometry = ip;
+  const hpt_ref_material* mp = nullptr;
+  if ((s = dev_upload(out, d.materials, (size_t)d.num_materials, &mp)) != HPT_OK) return s;
+  ds.materials = mp;
+  if ((s = dev_upload(out, d.lights, 4 * (size_t)d.num_lights, &ip)) != HPT_OK) return s;
+  ds.lights = ip;
+  std::vector<DevTexInfo> ti(d.num_textures);
+  int64_t texels = 0;
+  for (int t = 0; t < d.num_textures; ++t) {
+    ti[t].offset = texels;
+    ti[t].w = d.texture_dims ? d.texture_dims[2 * t] : 512;
+    ti[t].h = d.texture_dims ? d.texture_dims[2 * t + 1] : 512;
+    texels += (int64_t)ti[t].w * ti[t].h;
+  }
+  const uint32_t* tx = nullptr;
+  if ((s = dev_upload(out, reinterpret_cast<const uint32_t*>(d.texture_data), (size_t)texels, &tx)) != HPT_OK)
+    return s;
+  ds.texels = tx;
+  const DevTexInfo* tip = nullptr;
+  if ((s = dev_upload(out, ti.data(), ti.size(), &tip)) != HPT_OK) return s;
+  ds.tex_info = tip;
+  ds.num_nodes = (int32_t)pk.nodes.size();
+  ds.num_leaves = (int32_t)pk.leaves.size();
+  ds.num_leaf_tris = (int32_t)pk.refs.size();
+  ds.num_triangles = d.num_triangles;
+  ds.num_points = d.num_points;
+  ds.num_normals = d.num_normals;
+  ds.num_texcoords = d.num_texcoords;
+  ds.num_materials = d.num_materials;
+  ds.num_lights = d.num_lights;
+  ds.num_textures = d.num_textures;
+  float scale = 0.f;
+  for (int a = 0; a < 3; ++a) {
+    ds.root_lo[a] = pk.root_lo[a];
+    ds.root_hi[a] = pk.root_hi[a];
+    scale = std::max({scale, std::fabs(pk.root_lo[a]), std::fabs(pk.root_hi[a]),
+                      pk.root_hi[a] - pk.root_lo[a]});
+  }
+  ds.scene_eps = 2e-5f * scale;
+  const int64_t cap = 8 * ((int64_t)pk.nodes.size() + (int64_t)pk.refs.size()) + 100000;
+  ds.max_steps = (int32_t)std::min<int64_t>(cap, 1 << 30);
+  void* p = nullptr;
+  HPT_CUDA(cudaMalloc(&p, sizeof(DevScene)));
+  out.allocations.push_back(p);
+  HPT_CUDA(cudaMemcpy(p, &ds, sizeof(DevScene), cudaMemcpyHostToDevice));
+  out.d_scene = static_cast<DevScene*>(p);
+  out.info.num_triangles = d.num_triangles;
+  out.info.num_ref_nodes = d.num_nodes;
+  out.info.num_device_nodes = ds.num_nodes;
+  out.info.num_leaves = ds.num_leaves;
+  out.info.num_leaf_triangles = (int32_t)pk.refs.size();
+  out.info.max_depth = pk.max_depth;
+  out.info.device_bytes = out.bytes;
+  return HPT_OK;
+}
+
+void release_scene(SceneDev& s) {
+  cudaSetDevice(s.device);
+  for (void* p : s.allocations) cudaFree(p);
+  s.allocations.clear();
+}
+
+}  // namespace hpt
+
+namespace {
+
+hpt_status check_params(const hpt_camera* cam, const hpt_render_params* p) {
+  if (!cam || !p) return fail(HPT_ERR_INVALID_ARGUMENT, "camera/params is NULL");
+  if (p->sample_x <= 0 || p->sample_y <= 0 || p->supersample_x <= 0 || p->supersample_y <= 0 ||
+      p->sample <= 0 || p->depth <= 0)
+    return fail(HPT_ERR_INVALID_ARGUMENT, "sizes, sample and depth must be positive");
+  const int64_t rays = (int64_t)p->sample_x * p->supersample_x * p->sample_y * p->supersample_y;
+  if (rays > (1ll << 31) - 1) return fail(HPT_ERR_INVALID_ARGUMENT, "too many rays per frame");
+  if (p->sample >= (1 << 24)) return fail(HPT_ERR_INVALID_ARGUMENT, "sample must be < 2^24");
+  if (p->depth > 255) return fail(HPT_ERR_INVALID_ARGUMENT, "depth must be <= 255");
+  if (cam->height < 0 && p->supersample_x != p->supersample_y)
+    return fail(HPT_ERR_INVALID_ARGUMENT,
+                "panorama needs supersample_x == supersample_y (the reference indexes rays with "
+                "sample_x * supersample_y)");
+  return HPT_OK;
+}
+
+template <typename F>
+hpt_status guarded(F&& f) {
+  try {
+    return f();
+  } catch (const std::bad_alloc&) {
+    return fail(HPT_ERR_OUT_OF_MEMORY, "host allocation failed");
+  } catch (...) {
+    return fail(HPT_ERR_INVALID_ARGUMENT, "unexpected exception");
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int hpt_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+hpt_status hpt_scene_create(const hpt_scene_desc* desc, hpt_scene** out) {
+  if (!desc || !out) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  return guarded([&]() -> hpt_status {
+    std::unique_ptr<hpt_scene> s(new hpt_scene());
+    hpt_status st = upload_scene(*desc, s->h.scene);
+    if (st != HPT_OK) {
+      release_scene(s->h.scene);
+      return st;
+    }
+    s->h.tuning = default_tuning();
+    *out = s.release();
+    return HPT_OK;
+  });
+}
+
+hpt_status hpt_scene_info_get(const hpt_scene* scene, hpt_scene_info* out) {
+  if (!scene || !out) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  *out = scene->h.scene.info;
+  return HPT_OK;
+}
+
+void hpt_scene_destroy(hpt_scene* scene) {
+  if (!scene) return;
+  {
+    std::lock_guard<std::mutex> lk(scene->h.mu);
+    scene->h.engine.reset();
+    release_scene(scene->h.scene);
+  }
+  delete scene;
+}
+
+hpt_status hpt_render(hpt_scene* scene, const hpt_camera* camera, const hpt_render_params* params,
+                      uint8_t* rgba_out, float* accum_out) {
+  if (!scene) return fail(HPT_ERR_INVALID_ARGUMENT, "scene is NULL");
+  hpt_status s = check_params(camera, params);
+  if (s != HPT_OK) return s;
+  return guarded([&]() -> hpt_status {
+    std::lock_guard<std::mutex> lk(scene->h.mu);
+    if (!scene->h.engine) scene->h.engine.reset(new Engine(scene->h.scene.device));
+    scene->h.engine->tuning = scene->h.tuning;
+    JobSpec js;
+    js.scene = &scene->h.scene;
+    js.camera = *camera;
+    js.params = *params;
+    js.rgba_out = rgba_out;
+    js.accum_out = accum_out;
+    return scene->h.engine->run({js}, &scene->h.last_stats);
+  });
+}
+
+hpt_status hpt_render_stats_get(const hpt_scene* scene, hpt_render_stats* out) {
+  if (!scene || !out) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  *out = scene->h.last_stats;
+  return HPT_OK;
+}
+
+hpt_status hpt_tuning_get(const hpt_scene* scene, hpt_tuning* out) {
+  if (!scene || !out) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  *out = scene->h.tuning;
+  return HPT_OK;
+}
+
+hpt_status hpt_tuning_set(hpt_scene* scene, const hpt_tuning* in) {
+  if (!scene || !in) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (in->capacity < 1024 || in->capacity > (1 << 27) || in->smem_nodes < 0 ||
+      in->smem_nodes > 8192 || in->refill_chunk < 1 || in->refill_chunk > 32)
+    return fail(HPT_ERR_INVALID_ARGUMENT, "tuning out of range");
+  std::lock_guard<std::mutex> lk(scene->h.mu);
+  scene->h.tuning = *in;
+  scene->h.tuning.isect_block = 256;
+  scene->h.tuning.shade_block = 256;
+  scene->h.engine.reset();
+  return HPT_OK;
+}
+
+hpt_status hpt_raygen(const hpt_camera* camera, int32_t sample_x, int32_t sample_y,
+                      int32_t supersample_x, int32_t supersample_y, float* origins,
+                      float* directions) {
+  if (!camera || !origins || !directions || sample_x <= 0 || sample_y <= 0 || supersample_x <= 0 ||
+      supersample_y <= 0)
+    return fail(HPT_ERR_INVALID_ARGUMENT, "bad raygen arguments");
+  if (camera->height < 0 && supersample_x != supersample_y)
+    return fail(HPT_ERR_INVALID_ARGUMENT, "panorama needs supersample_x == supersample_y");
+  return guarded([&]() -> hpt_status {
+    const int nx = sample_x * supersample_x, ny = sample_y * supersample_y;
+    const size_t bytes = (size_t)nx * ny * 3 * sizeof(float);
+    DBuf o, d;
+    hpt_status s;
+    if ((s = o.alloc(bytes)) != HPT_OK || (s = d.alloc(bytes)) != HPT_OK) return s;
+    const int pano = camera->height < 0;
+    const int shift = (int)camera->right_dir[0] * supersample_x;
+    dim3 blk(16, 16), grd((nx + 15) / 16, (ny + 15) / 16);
+    k_stage_raygen<<<grd, blk>>>(*camera, nx, ny, pano, shift, o.as<float>(), d.as<float>());
+    HPT_CUDA(cudaGetLastError());
+    if ((s = o.down(origins)) != HPT_OK) return s;
+    return d.down(directions);
+  });
+}
+
+hpt_status hpt_intersect(hpt_scene* scene, int32_t n, const float* origins,
+                         const float* directions, int32_t* tri_out, float* t_out, float* u_out,
+                         float* v_out) {
+  if (!scene || n < 0 || (n > 0 && (!origins || !directions || !tri_out || !t_out || !u_out || !v_out)))
+    return fail(HPT_ERR_INVALID_ARGUMENT, "bad intersect arguments");
+  if (n == 0) return HPT_OK;
+  return guarded([&]() -> hpt_status {
+    std::lock_guard<std::mutex> lk(scene->h.mu);
+    HPT_CUDA(cudaSetDevice(scene->h.scene.device));
+    DBuf o, d, tri, t, u, v, err;
+    hpt_status s;
+    const size_t b3 = (size_t)n * 3 * sizeof(float), b1 = (size_t)n * 4;
+    if ((s = o.up(origins, b3)) || (s = d.up(directions, b3)) || (s = tri.alloc(b1)) ||
+        (s = t.alloc(b1)) || (s = u.alloc(b1)) || (s = v.alloc(b1)) || (s = err.alloc(4)))
+      return s;
+    HPT_CUDA(cudaMemset(err.p, 0, 4));
+    k_stage_intersect<<<blocks_for(n, 128), 128>>>(scene->h.scene.d_scene, n, o.as<float>(),
+                                                   d.as<float>(), tri.as<int32_t>(), t.as<float>(),
+                                                   u.as<float>(), v.as<float>(), err.as<uint32_t>());
+    HPT_CUDA(cudaGetLastError());
+    uint32_t e = 0;
+    if ((s = tri.down(tri_out)) || (s = t.down(t_out)) || (s = u.down(u_out)) || (s = v.down(v_out)) ||
+        (s = err.down(&e)))
+      return s;
+    if (e) return fail(HPT_ERR_TRAVERSAL_LIMIT, "a traversal hit its step cap");
+    return HPT_OK;
+  });
+}
+
+hpt_status hpt_shade(hpt_scene* scene, int32_t n, const float* origins, const float* directions,
+                     const float* strengths, const int32_t* tris, const float* ts, uint64_t* seeds,
+                     int32_t disable_diffuse, float* contrib, int32_t* branch, float* hit_p,
+                     float* normal, float* strength_out, float* param) {
+  if (!scene || n < 0 ||
+      (n > 0 && (!origins || !directions || !strengths || !tris || !ts || !seeds || !contrib ||
+                 !branch || !hit_p || !normal || !strength_out || !param)))
+    return fail(HPT_ERR_INVALID_ARGUMENT, "bad shade arguments");
+  if (n == 0) return HPT_OK;
+  for (int i = 0; i < n; ++i)
+    if (tris[i] < 0 || tris[i] >= scene->h.scene.info.num_triangles)
+      return fail(HPT_ERR_INVALID_ARGUMENT, "shade: triangle id %d out of range", tris[i]);
+  return guarded([&]() -> hpt_status {
+    std::lock_guard<std::mutex> lk(scene->h.mu);
+    HPT_CUDA(cudaSetDevice(scene->h.scene.device));
+    const size_t b3 = (size_t)n * 3 * sizeof(float), b1 = (size_t)n * 4, b8 = (size_t)n * 8;
+    DBuf o, d, st, tri, t, sd, co, br, hp, nm, so, pa;
+    hpt_status s;
+    if ((s = o.up(origins, b3)) || (s = d.up(directions, b3)) || (s = st.up(strengths, b3)) ||
+        (s = tri.up(tris, b1)) || (s = t.up(ts, b1)) || (s = sd.up(seeds, b8)) ||
+        (s = co.alloc(b3)) || (s = br.alloc(b1)) || (s = hp.alloc(b3)) || (s = nm.alloc(b3)) ||
+        (s = so.alloc(b3)) || (s = pa.alloc(b1)))
+      return s;
+    k_stage_shade<<<blocks_for(n, 128), 128>>>(
+        scene->h.scene.d_scene, n, o.as<float>(), d.as<float>(), st.as<float>(), tri.as<int32_t>(),
+        t.as<float>(), sd.as<uint64_t>(), disable_diffuse, co.as<float>(), br.as<int32_t>(),
+        hp.as<float>(), nm.as<float>(), so.as<float>(), pa.as<float>());
+    HPT_CUDA(cudaGetLastError());
+    if ((s = sd.down(seeds)) || (s = co.down(contrib)) || (s = br.down(branch)) ||
+        (s = hp.down(hit_p)) || (s = nm.down(normal)) || (s = so.down(strength_out)) ||
+        (s = pa.down(param)))
+      return s;
+    return HPT_OK;
+  });
+}
+
+hpt_status hpt_next_dir(hpt_scene* scene, int32_t n, const int32_t* branch,
+                        const float* directions, const float* hit_p, const float* normal,
+                        const float* strengths, const float* param, uint64_t* seeds,
+                        float* origins_out, float* directions_out, float* strength_out,
+                        int32_t* alive_out) {
+  if (!scene || n < 0 ||
+      (n > 0 && (!branch || !directions || !hit_p || !normal || !strengths || !param || !seeds ||
+                 !origins_out || !directions_out || !strength_out || !alive_out)))
+    return fail(HPT_ERR_INVALID_ARGUMENT, "bad next_dir arguments");
+  if (n == 0) return HPT_OK;
+  return guarded([&]() -> hpt_status {
+    std::lock_guard<std::mutex> lk(scene->h.mu);
+    HPT_CUDA(cudaSetDevice(scene->h.scene.device));
+    const size_t b3 = (size_t)n * 3 * sizeof(float), b1 = (size_t)n * 4, b8 = (size_t)n * 8;
+    DBuf br, d, hp, nm, st, pa, sd, oo, dd, so, al;
+    hpt_status s;
+    if ((s = br.up(branch, b1)) || (s = d.up(directions, b3)) || (s = hp.up(hit_p, b3)) ||
+        (s = nm.up(normal, b3)) || (s = st.up(strengths, b3)) || (s = pa.up(param, b1)) ||
+        (s = sd.up(seeds, b8)) || (s = oo.alloc(b3)) || (s = dd.alloc(b3)) || (s = so.alloc(b3)) ||
+        (s = al.alloc(b1)))
+      return s;
+    k_stage_next<<<blocks_for(n, 128), 128>>>(scene->h.scene.d_scene, n, br.as<int32_t>(),
+                                              d.as<float>(), hp.as<float>(), nm.as<float>(),
+                                              st.as<float>(), pa.as<float>(), sd.as<uint64_t>(),
+                                              oo.as<float>(), dd.as<float>(), so.as<float>(),
+                                              al.as<int32_t>());
+    HPT_CUDA(cudaGetLastError());
+    if ((s = sd.down(seeds)) || (s = oo.down(origins_out)) || (s = dd.down(directions_out)) ||
+        (s = so.down(strength_out)) || (s = al.down(alive_out)))
+      return s;
+    return HPT_OK;
+  });
+}
+
+hpt_status hpt_compact(const uint32_t* flags, int32_t n, int32_t* out, int32_t* count) {
+  if (n < 0 || !count || (n > 0 && (!flags || !out)))
+    return fail(HPT_ERR_INVALID_ARGUMENT, "bad compact arguments");
+  *count = 0;
+  if (n == 0) return HPT_OK;
+  if (hpt_device_count() == 0) return fail(HPT_ERR_CUDA, "no CUDA device");
+  return guarded([&]() -> hpt_status {
+    const int nb = blocks_for(n, kCompactTile);
+    DBuf f, o, bc, tot;
+    hpt_status s;
+    if ((s = f.up(flags, (size_t)n * 4)) || (s = o.alloc((size_t)n * 4)) ||
+        (s = bc.alloc((size_t)nb * 4)) || (s = tot.alloc(4)))
+      return s;
+    k_compact_count<<<nb, kCompactThreads>>>(f.as<uint32_t>(), n, bc.as<int>());
+    k_compact_scan<<<1, 1024>>>(bc.as<int>(), nb, tot.as<int>());
+    k_compact_scatter<<<nb, kCompactThreads>>>(f.as<uint32_t>(), n, bc.as<int>(), o.as<int>());
+    HPT_CUDA(cudaGetLastError());
+    int total = 0;
+    if ((s = tot.down(&total))) return s;
+    if (total > 0) HPT_CUDA(cudaMemcpy(out, o.p, (size_t)total * 4, cudaMemcpyDeviceToHost));
+    *count = total;
+    return HPT_OK;
+  });
+}
+
+hpt_status hpt_resolve(const float* accum, int32_t sample_x, int32_t sample_y, int32_t supersample_x,
+                       int32_t supersample_y, int32_t sample, float brightness, uint8_t* rgba_out) {
+  if (!accum || !rgba_out || sample_x <= 0 || sample_y <= 0 || supersample_x <= 0 ||
+      supersample_y <= 0 || sample <= 0)
+    return fail(HPT_ERR_INVALID_ARGUMENT, "bad resolve arguments");
+  if (hpt_device_count() == 0) return fail(HPT_ERR_CUDA, "no CUDA device");
+  return guarded([&]() -> hpt_status {
+    const size_t rays = (size_t)sample_x * supersample_x * sample_y * supersample_y;
+    DBuf a, o;
+    hpt_status s;
+    if ((s = a.up(accum, rays * 3 * sizeof(float))) || (s = o.alloc((size_t)sample_x * sample_y * 4)))
+      return s;
+    dim3 blk(16, 16), grd((sample_x + 15) / 16, (sample_y + 15) / 16);
+    k_stage_resolve<<<grd, blk>>>(a.as<float>(), sample_x, sample_y, supersample_x, supersample_y,
+                                  sample, brightness, o.as<uint8_t>());
+    HPT_CUDA(cudaGetLastError());
+    return o.down(rgba_out);
+  });
+}
+
+// --- Batching ---------------------------------------------------------------
+
+struct hpt_batch {
+  int device;
+  std::unique_ptr<Engine> engine;
+  std::vector<JobSpec> jobs;
+  hpt_render_stats stats{};
+  hpt_tuning tuning = default_tuning();
+};
+
+hpt_status hpt_batch_create(int32_t device, hpt_batch** out) {
+  if (!out) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  if (device < 0 || device >= hpt_device_count()) return fail(HPT_ERR_CUDA, "no CUDA device %d", device);
+  return guarded([&]() -> hpt_status {
+    hpt_batch* b = new hpt_batch();
+    b->device = device;
+    *out = b;
+    return HPT_OK;
+  });
+}
+
+hpt_status hpt_batch_add(hpt_batch* batch, hpt_scene* scene, const hpt_camera* camera,
+                         const hpt_render_params* params, uint8_t* rgba_out, float* accum_out,
+                         int32_t* job_id) {
+  if (!batch || !scene) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  hpt_status s = check_params(camera, params);
+  if (s != HPT_OK) return s;
+  if (scene->h.scene.device != batch->device)
+    return fail(HPT_ERR_INVALID_ARGUMENT, "scene lives on another device");
+  JobSpec js;
+  js.scene = &scene->h.scene;
+  js.camera = *camera;
+  js.params = *params;
+  js.rgba_out = rgba_out;
+  js.accum_out = accum_out;
+  batch->jobs.push_back(js);
+  if (job_id) *job_id = (int32_t)batch->jobs.size() - 1;
+  return HPT_OK;
+}
+
+hpt_status hpt_batch_run(hpt_batch* batch) {
+  if (!batch) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  return guarded([&]() -> hpt_status {
+    if (!batch->engine) batch->engine.reset(new Engine(batch->device));
+    batch->engine->tuning = batch->tuning;
+    hpt_status s = batch->engine->run(batch->jobs, &batch->stats);
+    batch->jobs.clear();
+    return s;
+  });
+}
+
+hpt_status hpt_batch_stats_get(const hpt_batch* batch, hpt_render_stats* out) {
+  if (!batch || !out) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  *out = batch->stats;
+  return HPT_OK;
+}
+
+hpt_status hpt_batch_tuning_set(hpt_batch* batch, const hpt_tuning* in) {
+  if (!batch || !in) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  batch->tuning = *in;
+  batch->engine.reset();
+  return HPT_OK;
+}
+
+void hpt_batch_destroy(hpt_batch* batch) { delete batch; }
+
+}  // extern "C"

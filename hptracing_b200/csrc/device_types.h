@@ -1,0 +1,135 @@
+// Device-side scene and wavefront layouts, shared by the host packer (C++)
+// and the CUDA kernels. Plain structs only: no CUDA headers needed here.
+#pragma once
+
+#include <cstdint>
+
+namespace hpt {
+
+// --- Traversal tree ------------------------------------------------------
+// 8-byte node. meta bits 31..30: 0/1/2 = split axis of an inner node,
+// 3 = leaf. Inner nodes: bits 29..0 = index of the left child; the right
+// child is stored right after it. Leaves: bits 29..0 = leaf record index.
+// word 1: split position (inner) / unused (leaf).
+struct DevNode {
+  uint32_t meta;
+  float split;
+};
+static_assert(sizeof(DevNode) == 8, "8-byte traversal node");
+constexpr uint32_t kLeafKind = 3u;
+constexpr uint32_t kIndexMask = 0x3FFFFFFFu;
+
+// Leaf record, 64 bytes (4 x 16 B):
+//  [0] lo.x lo.y lo.z  first entry in leaf_refs (int bits)
+//  [1] hi.x hi.y hi.z  number of entries (int bits)
+//  [2] rope -x, +x, -y, +y   (node index, -1 = leaves the scene)
+//  [3] rope -z, +z, reference node index, 0
+// The box is the reference node's own box; ropes point to the smallest
+// node on the other side of each face that contains the whole face.
+struct DevLeaf {
+  float lo[3];
+  int32_t tri_begin;
+  float hi[3];
+  int32_t tri_count;
+  int32_t rope[6];
+  int32_t ref_node;
+  int32_t pad;
+};
+static_assert(sizeof(DevLeaf) == 64, "64-byte leaf record");
+
+// Triangle record, one per triangle, 48 bytes (3 x 16 B): vertex a,
+// e1 = b - a, e2 = c - a (computed in FP32 exactly as the reference's
+// _single_intersect does), triangle id and material in the .w slots.
+// Leaves reference triangles through 4-byte ids stored in the reference's
+// gather order (the reference duplicates a straddling triangle in every
+// leaf it touches - tens of references per triangle on its SAH trees - so
+// ids keep the records themselves small enough to stay in L2).
+struct DevTri {
+  float a[3];
+  int32_t tri_id;
+  float e1[3];
+  int32_t material;
+  float e2[3];
+  int32_t pad;
+};
+static_assert(sizeof(DevTri) == 48, "48-byte triangle record");
+
+// Per-texture descriptor: texel offset into the RGBA8 pool, width, height.
+struct DevTexInfo {
+  int64_t offset;
+  int32_t w, h;
+};
+
+// Pointers of one device-resident scene (all device addresses).
+struct DevScene {
+  const DevNode* nodes;
+  const DevLeaf* leaves;
+  const int32_t* leaf_refs;   // triangle ids in leaf (= reference gather) order
+  const DevTri* tris;         // indexed by triangle id
+  const float* points;      // float4 per vertex
+  const float* normals;     // float4 per vertex or null
+  const float* texcoords;   // float2 per vertex or null
+  const int32_t* geometry;  // int4 (v0, v1, v2, material) per triangle
+  const void* materials;    // hpt_ref_material[]
+  const int32_t* lights;    // int4 [num_lights]
+  const uint32_t* texels;   // RGBA8 pool
+  const DevTexInfo* tex_info;
+  int32_t num_nodes, num_leaves, num_leaf_tris, num_triangles;
+  int32_t num_points, num_normals, num_texcoords, num_materials;
+  int32_t num_lights, num_textures;
+  float root_lo[3], root_hi[3];
+  float scene_eps;          // termination slack in world units
+  int32_t max_steps;        // traversal step cap per ray
+};
+
+// --- Wavefront job table ------------------------------------------------
+struct DevJob {
+  DevScene scene;
+  float view_p[3], top[3], right[3];
+  float width, height;
+  int32_t nx, ny;           // rays per frame along x and y
+  int32_t pano;             // 1 = equirectangular (set_viewdirs_vr)
+  int32_t vr_x_shift;       // shift * supersample_x
+  int32_t vr_sample_x;      // sample_x * supersample_y (as the reference)
+  int32_t vr_sample_y;      // sample_y * supersample_y
+  float bg[3];
+  int32_t spp, depth, disable_diffuse;
+  uint64_t seed;
+  unsigned long long* accum;  // 3 x fixed-point u64 per ray
+  uint32_t* flags;          // per ray: NaN / +inf / -inf markers (4 bits per channel)
+  float* prim;              // primary hit cache, 8 floats per entry
+  int32_t* prim_count;      // number of primary hits
+  int64_t prim_base;        // first global primary ray of this job
+  int64_t path_base;        // first global path index (set on device)
+  int64_t num_paths;        // prim_count * spp (set on device)
+  unsigned long long* counters;  // [0] intersect queries [1] shades [2] paths done
+};
+
+// Wavefront control block (device memory, updated by the control kernel).
+struct DevCtrl {
+  int32_t nA;               // paths in the current shade queue
+  int32_t nR;               // rays in the intersect queue
+  int32_t nA_next;          // hits appended by the intersect kernel
+  int32_t isect_head;       // refill cursor of the intersect kernel
+  int32_t prim_head;        // refill cursor of the primary kernel
+  int32_t parity;           // which shade buffer is current
+  int32_t n_new;            // new paths started by the last shade pass
+  int32_t done;
+  int64_t cursor;           // next new path (global index)
+  int64_t total_paths;
+  int64_t iterations;
+  uint32_t error;           // bit 0: traversal step cap reached
+  uint32_t pad;
+  unsigned long long isect_queries;
+  unsigned long long shades;
+  unsigned long long nodes_visited;
+  unsigned long long leaves_visited;
+  unsigned long long tri_tests;
+};
+
+// Fixed-point scale of the per-ray accumulators (2^32): integer sums are
+// exact and order-independent, so a render is bit-reproducible no matter
+// how paths are scheduled.
+constexpr double kAccumScale = 4294967296.0;
+
+}  // namespace hpt

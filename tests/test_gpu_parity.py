@@ -1,0 +1,167 @@
+"""GPU kernels against the oracle (bit-exact where the reference arithmetic
+is + - * / sqrt only; a stated tolerance where OpenCL transcendentals are
+involved). Every call goes through the C ABI of libhpt.so."""
+import numpy as np
+import pytest
+
+import hptracing_b200 as H
+import oracle as O
+from tests import scenes as S
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def room(built):
+    if H.device_count() == 0:
+        pytest.skip("no CUDA device")
+    mesh, nodes, leaf = S.make_scene(0)
+    return mesh, H.Scene(mesh, nodes, leaf), O.CpuScene(mesh, nodes, leaf)
+
+
+@pytest.fixture(scope="module")
+def spheres(built):
+    if H.device_count() == 0:
+        pytest.skip("no CUDA device")
+    mesh, nodes, leaf = S.make_scene(1, seed=1, texture_size=128)
+    return mesh, H.Scene(mesh, nodes, leaf), O.CpuScene(mesh, nodes, leaf)
+
+
+def _rays(kind, n=50000):
+    if kind == "camera":
+        return O.raygen(S.ROOM_CAM, 256, 192, 1, 1)
+    if kind == "pano":
+        return O.raygen(S.PANO_CAM, 256, 128, 1, 1)
+    return S.random_rays(n, seed=11)
+
+
+def _check_intersect(gpu, cpu, o, d):
+    tri, t, u, v = gpu.intersect(o, d)
+    ref = cpu.intersect(o, d)
+    ok = ref["overflow"] == 0
+    mism = np.nonzero(ok & ((tri != ref["tri"]) | (t != ref["t"]) | (u != ref["u"]) |
+                            (v != ref["v"])))[0]
+    assert len(mism) == 0, "%d of %d rays differ, first %s: gpu %s ref %s" % (
+        len(mism), len(o), mism[:5], tri[mism[:5]], ref["tri"][mism[:5]])
+    return tri, ref
+
+
+@pytest.mark.parametrize("kind", ["camera", "pano", "random"])
+def test_intersect_bitexact_room(room, kind):
+    _, gpu, cpu = room
+    o, d = _rays(kind)
+    tri, _ = _check_intersect(gpu, cpu, o, d)
+    assert (tri >= 0).sum() > len(o) // 4
+
+
+@pytest.mark.parametrize("kind", ["camera", "random"])
+def test_intersect_bitexact_spheres(spheres, kind):
+    _, gpu, cpu = spheres
+    o, d = _rays(kind)
+    _check_intersect(gpu, cpu, o, d)
+
+
+def test_intersect_secondary_rays(spheres):
+    """Rays that start on surfaces (1e-5 off the hit point, as s2 emits)."""
+    _, gpu, cpu = spheres
+    o, d = _rays("random", 30000)
+    ref = cpu.intersect(o, d)
+    h = ref["tri"] >= 0
+    rng = np.random.default_rng(3)
+    p = o[h] + ref["t"][h, None] * d[h]
+    nd = rng.normal(size=p.shape).astype(np.float32)
+    nd /= np.linalg.norm(nd, axis=1, keepdims=True)
+    o2 = (p + np.float32(1e-5) * nd).astype(np.float32)
+    _check_intersect(gpu, cpu, o2, nd.astype(np.float32))
+
+
+def test_intersect_fp32_vs_fp64(room):
+    """States the FP32 hit-distance error against an FP64 brute force."""
+    _, gpu, cpu = room
+    o, d = _rays("random", 20000)
+    tri, t, _, _ = gpu.intersect(o, d)
+    btri, bt = cpu.brute_f64(o, d)
+    both = (tri >= 0) & (btri >= 0)
+    rel = np.abs(t[both] - bt[both]) / np.maximum(bt[both], 1e-6)
+    same = (tri == btri).mean()
+    print("fp32 vs fp64: same triangle %.5f, max rel t err %.3g, p99 %.3g"
+          % (same, rel.max(), np.percentile(rel, 99)))
+    assert same > 0.999
+    assert np.percentile(rel, 99) < 1e-5
+
+
+def _hits(cpu, n, seed):
+    o, d = S.random_rays(n, seed)
+    ref = cpu.intersect(o, d)
+    h = np.nonzero(ref["tri"] >= 0)[0]
+    rng = np.random.default_rng(seed + 1)
+    st = rng.uniform(0.0, 1.0, (len(h), 3)).astype(np.float32)
+    st[:50] = 1e-5  # some rays below the termination threshold
+    seeds = rng.integers(0, 2 ** 48, len(h), dtype=np.int64)
+    return o[h], d[h], st, ref["tri"][h], ref["t"][h], seeds
+
+
+@pytest.mark.parametrize("disable_diffuse", [0, 1])
+def test_shade_bitexact(spheres, disable_diffuse):
+    _, gpu, cpu = spheres
+    o, d, st, tri, t, seeds = _hits(cpu, 40000, 5)
+    g = gpu.shade(o, d, st, tri, t, seeds.astype(np.uint64), disable_diffuse)
+    r = cpu.shade(o, d, st, tri, t, seeds, disable_diffuse)
+    alive = r["branch"] >= 0
+    for k in ("contrib", "branch"):
+        assert np.array_equal(g[k], r[k]), k
+    for k in ("hit_p", "normal", "strength", "param"):
+        assert np.array_equal(g[k][alive], r[k][alive]), k
+    assert np.array_equal(g["seeds"].astype(np.int64)[alive], r["seeds"][alive])
+    assert len(np.unique(r["branch"])) >= 4
+
+
+def test_next_dir(spheres):
+    _, gpu, cpu = spheres
+    o, d, st, tri, t, seeds = _hits(cpu, 40000, 9)
+    r = cpu.shade(o, d, st, tri, t, seeds)
+    a = np.nonzero(r["branch"] >= 0)[0]
+    args = (r["branch"][a], d[a], r["hit_p"][a], r["normal"][a], r["strength"][a],
+            r["param"][a])
+    g = gpu.next_dir(*args, r["seeds"][a].astype(np.uint64))
+    c = cpu.next_dir(*args, r["seeds"][a])
+    br = r["branch"][a]
+    light = br == 3
+    # light branch: + - * / sqrt only -> bit-exact
+    for k in ("origins", "directions", "strength", "alive"):
+        assert np.array_equal(g[k][light], c[k][light]), k
+    # other branches use acos/sin/cos/pow/asin: agree to a few ulp
+    tol = 2e-5
+    for k in ("origins", "directions", "strength"):
+        err = np.abs(g[k][~light] - c[k][~light]) / np.maximum(np.abs(c[k][~light]), 1.0)
+        assert err.max() < tol, (k, err.max())
+    assert (g["alive"] == c["alive"]).mean() > 0.9999
+    assert np.array_equal(g["seeds"].astype(np.int64), c["seeds"])
+
+
+def test_raygen():
+    cam = S.hp_camera(S.ROOM_CAM)
+    o, d = H.raygen(cam, 96, 64, 2, 2)
+    ro, rd = O.raygen(S.ROOM_CAM, 96, 64, 2, 2)
+    assert np.array_equal(o, ro) and np.array_equal(d, rd)
+    pcam = S.hp_camera(S.PANO_CAM)
+    o, d = H.raygen(pcam, 96, 48, 2, 2)
+    ro, rd = O.raygen(S.PANO_CAM, 96, 48, 2, 2)
+    assert np.array_equal(o, ro)
+    assert np.abs(d - rd).max() < 2e-6
+
+
+def test_resolve():
+    rng = np.random.default_rng(1)
+    acc = rng.gamma(1.0, 3.0, (80 * 2 * 60 * 2, 3)).astype(np.float32)
+    g = H.resolve(acc, 80, 60, 2, 2, 16, 1.5)
+    r = O.resolve(acc, 80, 60, 2, 2, 16, 1.5)
+    assert np.abs(g.astype(int) - r.astype(int)).max() <= 1
+    assert (g != r).mean() < 0.01
+
+
+@pytest.mark.parametrize("n", [0, 1, 31, 2048, 100003, 3000000])
+def test_compact(n):
+    rng = np.random.default_rng(n)
+    f = (rng.random(n) < 0.37).astype(np.uint32)
+    assert np.array_equal(H.compact(f), np.nonzero(f)[0].astype(np.int32))
