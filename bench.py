@@ -40,6 +40,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # Overrides for profiling runs only (the headline workload is the default).
+    ap.add_argument("--res", type=int, default=0)
+    ap.add_argument("--spp", type=int, default=0)
     return ap.parse_args()
 
 
@@ -210,7 +213,12 @@ def run_reference(args):
 
 
 def main():
+    global W_RES, H_RES, SPP, WORKLOAD
     args = parse()
+    if args.res or args.spp:
+        W_RES = H_RES = args.res or W_RES
+        SPP = args.spp or SPP
+        WORKLOAD = "profiling_case_%dx%d_spp%d_d%d" % (W_RES, H_RES, SPP, DEPTH)
     if args.impl == "reference":
         run_reference(args)
         return

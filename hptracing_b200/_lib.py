@@ -9,7 +9,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libhpt.so")
+# HPT_LIBRARY selects another build of the same ABI (e.g. a diagnostic one).
+LIB_PATH = os.environ.get("HPT_LIBRARY") or os.path.join(HERE, "libhpt.so")
 
 i32, i64, u64, f32, f64 = C.c_int32, C.c_int64, C.c_uint64, C.c_float, C.c_double
 P = C.POINTER
@@ -86,13 +87,13 @@ class RenderStats(C.Structure):
                 ("paths", i64), ("iterations", i32), ("error_flags", i32), ("ms_total", f32),
                 ("ms_primary", f32), ("ms_shade", f32), ("ms_intersect", f32),
                 ("ms_resolve", f32), ("ms_loop", f32), ("nodes_visited", i64),
-                ("leaves_visited", i64), ("triangle_tests", i64)]
+                ("leaves_visited", i64), ("triangle_tests", i64), ("triangle_repeats", i64)]
 
 
 class Tuning(C.Structure):
     _fields_ = [("capacity", i32), ("isect_block", i32), ("shade_block", i32),
                 ("refill_chunk", i32), ("smem_nodes", i32), ("use_graph", i32),
-                ("profile", i32), ("reserved", i32)]
+                ("profile", i32), ("isect_min_blocks", i32)]
 
 
 class ServerConfig(C.Structure):

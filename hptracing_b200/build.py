@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libhpt.so")
+CLI = os.path.join(HERE, "hptracing")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
@@ -48,19 +49,38 @@ def _newest_header():
     return t
 
 
-def _compile(src, verbose):
-    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+def _compile(src, verbose, build_dir=None, extra=()):
+    build_dir = build_dir or BUILD
+    obj = os.path.join(build_dir, os.path.basename(src) + ".o")
     hdr = _newest_header()
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr):
         return obj
-    cmd = [nvcc()] + COMMON + (CUDA_FLAGS if src.endswith(".cu") else ["-x", "c++"]) + [
-        "-c", src, "-o", obj]
+    cmd = [nvcc()] + COMMON + list(extra) + (
+        CUDA_FLAGS if src.endswith(".cu") else ["-x", "c++"]) + ["-c", src, "-o", obj]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("compile failed: %s\n%s%s" % (src, r.stdout, r.stderr))
     return obj
+
+
+def build_cli(verbose=False):
+    """The headless hptracing command line tool (C++, on the drop-in header)."""
+    src = os.path.join(HERE, "cli", "hptracing.cpp")
+    hdr = os.path.join(HERE, "..", "include", "hpt_trace_runner.hpp")
+    if (os.path.exists(CLI) and os.path.getmtime(CLI) >= max(os.path.getmtime(src),
+                                                             os.path.getmtime(hdr),
+                                                             os.path.getmtime(LIB))):
+        return CLI
+    cmd = ["g++", "-O2", "-std=c++14", "-I", os.path.join(HERE, "..", "include"), src, "-o", CLI,
+           "-L", HERE, "-lhpt", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("cli build failed\n%s%s" % (r.stdout, r.stderr))
+    return CLI
 
 
 def build(verbose=False, force=False):
@@ -73,6 +93,7 @@ def build(verbose=False, force=False):
         objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
     newest = max(os.path.getmtime(o) for o in objs)
     if os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
+        build_cli(verbose)
         return LIB
     cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lpthread"]
     if verbose:
@@ -80,7 +101,25 @@ def build(verbose=False, force=False):
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("link failed\n%s%s" % (r.stdout, r.stderr))
+    build_cli(verbose)
     return LIB
+
+
+def build_checked(verbose=False):
+    """libhpt_check.so: the same sources with every device index range-checked
+    (-DHPT_DEVICE_CHECKS); a failing check is reported as an error status
+    naming its site instead of touching memory. For diagnosis only."""
+    bdir = os.path.join(HERE, "_build_check")
+    os.makedirs(bdir, exist_ok=True)
+    out = os.path.join(HERE, "libhpt_check.so")
+    srcs = _sources()
+    with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        objs = list(ex.map(lambda s: _compile(s, verbose, bdir, ["-DHPT_DEVICE_CHECKS"]), srcs))
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", out] + objs + ["-lcudart", "-lpthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("link failed\n%s%s" % (r.stdout, r.stderr))
+    return out
 
 
 if __name__ == "__main__":

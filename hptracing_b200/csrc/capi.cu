@@ -40,7 +40,7 @@ struct DBuf {
   void* p = nullptr;
   size_t bytes = 0;
   ~DBuf() {
-    if (p) cudaFree(p);
+    if (p) HPT_SOFT(cudaFree(p));
   }
   hpt_status alloc(size_t b) {
     bytes = b;
@@ -69,14 +69,14 @@ struct DBuf {
 // Stage kernels (one thread per element).
 // ---------------------------------------------------------------------------
 __global__ void k_stage_intersect(const DevScene* s, int n, const float* o, const float* d,
-                                  int32_t* tri, float* t, float* u, float* v, uint32_t* err) {
+                                  int32_t* tri, float* t, float* u, float* v, DevErr* err) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   TravState st;
   trav_init(*s, Ray{mk(o[3 * i], o[3 * i + 1], o[3 * i + 2]), mk(d[3 * i], d[3 * i + 1], d[3 * i + 2])},
             st);
   TravCount cnt;
-  while (!trav_leaf(*s, st, nullptr, 0, err, cnt)) {
+  while (!trav_leaf<true>(*s, st, nullptr, 0, err, cnt)) {
   }
   tri[i] = st.best.tri;
   t[i] = st.best.rec >= 0 ? st.best.t : 0.f;
@@ -381,6 +381,11 @@ hpt_status upload_scene(const hpt_scene_desc& d, SceneDev& out) {
   HPT_CUDA(cudaMalloc(&p, sizeof(DevScene)));
   out.allocations.push_back(p);
   HPT_CUDA(cudaMemcpy(p, &ds, sizeof(DevScene), cudaMemcpyHostToDevice));
+  // A cudaMemcpy from pageable memory may return before its DMA has landed,
+  // and the render engines run on non-blocking streams that are not ordered
+  // after the legacy stream: wait here so no kernel can read a partially
+  // uploaded scene.
+  HPT_CUDA(cudaDeviceSynchronize());
   out.d_scene = static_cast<DevScene*>(p);
   out.info.num_triangles = d.num_triangles;
   out.info.num_ref_nodes = d.num_nodes;
@@ -393,8 +398,8 @@ hpt_status upload_scene(const hpt_scene_desc& d, SceneDev& out) {
 }
 
 void release_scene(SceneDev& s) {
-  cudaSetDevice(s.device);
-  for (void* p : s.allocations) cudaFree(p);
+  HPT_SOFT(cudaSetDevice(s.device));
+  for (void* p : s.allocations) HPT_SOFT(cudaFree(p));
   s.allocations.clear();
 }
 
@@ -402,20 +407,19 @@ void release_scene(SceneDev& s) {
 
 namespace {
 
-hpt_status check_params(const hpt_camera* cam, const hpt_render_params* p) {
-  if (!cam || !p) return fail(HPT_ERR_INVALID_ARGUMENT, "camera/params is NULL");
-  if (p->sample_x <= 0 || p->sample_y <= 0 || p->supersample_x <= 0 || p->supersample_y <= 0 ||
-      p->sample <= 0 || p->depth <= 0)
-    return fail(HPT_ERR_INVALID_ARGUMENT, "sizes, sample and depth must be positive");
-  const int64_t rays = (int64_t)p->sample_x * p->supersample_x * p->sample_y * p->supersample_y;
-  if (rays > (1ll << 31) - 1) return fail(HPT_ERR_INVALID_ARGUMENT, "too many rays per frame");
-  if (p->sample >= (1 << 24)) return fail(HPT_ERR_INVALID_ARGUMENT, "sample must be < 2^24");
-  if (p->depth > 255) return fail(HPT_ERR_INVALID_ARGUMENT, "depth must be <= 255");
-  if (cam->height < 0 && p->supersample_x != p->supersample_y)
-    return fail(HPT_ERR_INVALID_ARGUMENT,
-                "panorama needs supersample_x == supersample_y (the reference indexes rays with "
-                "sample_x * supersample_y)");
+// Ranges the engine supports (capacity: queue entries; smem_nodes: shared
+// node prefix; isect_block / isect_min_blocks: a compiled traversal variant,
+// 0 min blocks = the block size's default).
+hpt_status check_tuning(const hpt_tuning& t) {
+  if (t.capacity < 1024 || t.capacity > (1 << 27) || t.smem_nodes < 0 ||
+      t.smem_nodes > kMaxSmemNodes || t.refill_chunk < 1 || t.refill_chunk > 32 ||
+      (t.isect_block != 128 && t.isect_block != 256) || t.isect_min_blocks < 0)
+    return fail(HPT_ERR_INVALID_ARGUMENT, "tuning out of range");
   return HPT_OK;
+}
+
+hpt_status check_params(const hpt_camera* cam, const hpt_render_params* p) {
+  return check_render_params(cam, p);
 }
 
 template <typename F>
@@ -435,7 +439,10 @@ extern "C" {
 
 int hpt_device_count(void) {
   int n = 0;
-  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    (void)cudaGetLastError();  // "no device" is an answer here, not an error
+    return 0;
+  }
   return n;
 }
 
@@ -504,12 +511,10 @@ hpt_status hpt_tuning_get(const hpt_scene* scene, hpt_tuning* out) {
 
 hpt_status hpt_tuning_set(hpt_scene* scene, const hpt_tuning* in) {
   if (!scene || !in) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
-  if (in->capacity < 1024 || in->capacity > (1 << 27) || in->smem_nodes < 0 ||
-      in->smem_nodes > 8192 || in->refill_chunk < 1 || in->refill_chunk > 32)
-    return fail(HPT_ERR_INVALID_ARGUMENT, "tuning out of range");
+  hpt_status st = check_tuning(*in);
+  if (st != HPT_OK) return st;
   std::lock_guard<std::mutex> lk(scene->h.mu);
   scene->h.tuning = *in;
-  scene->h.tuning.isect_block = 256;
   scene->h.tuning.shade_block = 256;
   scene->h.engine.reset();
   return HPT_OK;
@@ -552,18 +557,22 @@ hpt_status hpt_intersect(hpt_scene* scene, int32_t n, const float* origins,
     hpt_status s;
     const size_t b3 = (size_t)n * 3 * sizeof(float), b1 = (size_t)n * 4;
     if ((s = o.up(origins, b3)) || (s = d.up(directions, b3)) || (s = tri.alloc(b1)) ||
-        (s = t.alloc(b1)) || (s = u.alloc(b1)) || (s = v.alloc(b1)) || (s = err.alloc(4)))
+        (s = t.alloc(b1)) || (s = u.alloc(b1)) || (s = v.alloc(b1)) ||
+        (s = err.alloc(sizeof(DevErr))))
       return s;
-    HPT_CUDA(cudaMemset(err.p, 0, 4));
+    HPT_CUDA(cudaMemset(err.p, 0, sizeof(DevErr)));
     k_stage_intersect<<<blocks_for(n, 128), 128>>>(scene->h.scene.d_scene, n, o.as<float>(),
                                                    d.as<float>(), tri.as<int32_t>(), t.as<float>(),
-                                                   u.as<float>(), v.as<float>(), err.as<uint32_t>());
+                                                   u.as<float>(), v.as<float>(), err.as<DevErr>());
     HPT_CUDA(cudaGetLastError());
-    uint32_t e = 0;
+    DevErr e;
     if ((s = tri.down(tri_out)) || (s = t.down(t_out)) || (s = u.down(u_out)) || (s = v.down(v_out)) ||
         (s = err.down(&e)))
       return s;
-    if (e) return fail(HPT_ERR_TRAVERSAL_LIMIT, "a traversal hit its step cap");
+    if (e.flags & 2u)
+      return fail(HPT_ERR_INVALID_SCENE, "device self-check %d failed (value %lld)", e.site,
+                  (long long)e.value);
+    if (e.flags) return fail(HPT_ERR_TRAVERSAL_LIMIT, "a traversal hit its step cap");
     return HPT_OK;
   });
 }
@@ -743,7 +752,10 @@ hpt_status hpt_batch_stats_get(const hpt_batch* batch, hpt_render_stats* out) {
 
 hpt_status hpt_batch_tuning_set(hpt_batch* batch, const hpt_tuning* in) {
   if (!batch || !in) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  hpt_status st = check_tuning(*in);
+  if (st != HPT_OK) return st;
   batch->tuning = *in;
+  batch->tuning.shade_block = 256;
   batch->engine.reset();
   return HPT_OK;
 }

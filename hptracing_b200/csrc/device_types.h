@@ -83,15 +83,15 @@ struct DevScene {
 };
 
 // --- Wavefront job table ------------------------------------------------
+// One render job (a frame of one scene) in a slot of the engine's table.
+// Read-only while the job runs; its mutable scheduling state is DevSlot.
 struct DevJob {
   DevScene scene;
   float view_p[3], top[3], right[3];
   float width, height;
   int32_t nx, ny;           // rays per frame along x and y
   int32_t pano;             // 1 = equirectangular (set_viewdirs_vr)
-  int32_t vr_x_shift;       // shift * supersample_x
-  int32_t vr_sample_x;      // sample_x * supersample_y (as the reference)
-  int32_t vr_sample_y;      // sample_y * supersample_y
+  int32_t vr_x_shift;       // int(right.x) * supersample_x
   float bg[3];
   int32_t spp, depth, disable_diffuse;
   uint64_t seed;
@@ -99,10 +99,25 @@ struct DevJob {
   uint32_t* flags;          // per ray: NaN / +inf / -inf markers (4 bits per channel)
   float* prim;              // primary hit cache, 8 floats per entry
   int32_t* prim_count;      // number of primary hits
-  int64_t prim_base;        // first global primary ray of this job
-  int64_t path_base;        // first global path index (set on device)
-  int64_t num_paths;        // prim_count * spp (set on device)
-  unsigned long long* counters;  // [0] intersect queries [1] shades [2] paths done
+};
+
+// Scheduling state of a slot. A job's paths are (primary hit k, sample s)
+// pairs enumerated as q = s * hits + k; `cursor` is the next q to start.
+struct DevSlot {
+  int64_t num_paths;        // hits * spp, set after the primary pass
+  int64_t cursor;
+  unsigned long long done;  // paths finished (flushed)
+  int32_t alloc;            // new paths granted for the coming shade pass
+  int32_t active;           // admitted and not yet fully issued
+};
+
+// Error word shared by the kernels. flags bit 0: a traversal hit its step
+// cap; bit 1: a device self-check failed (builds with HPT_DEVICE_CHECKS),
+// in which case site / value describe the first failure.
+struct DevErr {
+  uint32_t flags;
+  int32_t site;
+  long long value;
 };
 
 // Wavefront control block (device memory, updated by the control kernel).
@@ -113,18 +128,25 @@ struct DevCtrl {
   int32_t isect_head;       // refill cursor of the intersect kernel
   int32_t prim_head;        // refill cursor of the primary kernel
   int32_t parity;           // which shade buffer is current
-  int32_t n_new;            // new paths started by the last shade pass
-  int32_t done;
-  int64_t cursor;           // next new path (global index)
-  int64_t total_paths;
+  int32_t n_new;            // new paths granted to the coming shade pass
+  int32_t done;             // no queued path and nothing left to issue
+  int32_t n_quota;          // slots with a grant (quota_slot / quota_prefix)
+  int32_t n_order;          // slots in priority order (host-written)
   int64_t iterations;
-  uint32_t error;           // bit 0: traversal step cap reached
-  uint32_t pad;
+  DevErr err;
   unsigned long long isect_queries;
   unsigned long long shades;
   unsigned long long nodes_visited;
   unsigned long long leaves_visited;
   unsigned long long tri_tests;
+  unsigned long long tri_repeats;
+  // Self-check builds only: items the shade / intersect passes of the
+  // current iteration actually processed, compared by the control kernel
+  // with the queue sizes.
+  int32_t chk_shade_items;
+  int32_t chk_shade_done;
+  int32_t chk_isect_done;
+  int32_t chk_pad;
 };
 
 // Fixed-point scale of the per-ray accumulators (2^32): integer sums are

@@ -6,27 +6,33 @@
 // re-intersected up to `depth` shading passes, with blocking host reads of
 // the stage sizes after every stage.
 //
-// Here the same per-path arithmetic runs as a regenerating wavefront:
-//   k_primary  - ray generation + closest hit for every primary ray of every
-//                job; hits go to a per-job cache, misses write background.
+// Here the same per-path arithmetic runs as a regenerating wavefront over
+// job slots (one job = one frame of one scene):
+//   k_primary  - ray generation + closest hit for the primary rays of newly
+//                admitted jobs; hits go to a per-job cache, misses write
+//                background * sample.
+//   k_admit    - sets each new job's path count and grants paths.
 //   k_shade    - for each pending hit: self-emission, normal / UV / texture,
 //                branch choice and next direction (s1_run + s2_*_run fused);
 //                new (primary hit, sample) paths are started in the same
-//                pass until the wavefront is full. Survivors are compacted
-//                (warp ballot + block scan, one atomic per block) into the
-//                intersect queue; finished paths flush their radiance.
+//                pass from the grants. Survivors are compacted (warp ballot
+//                + block scan, one atomic per block) into the intersect
+//                queue; finished paths flush their radiance.
 //   k_isect    - closest hit for the intersect queue with persistent warps
 //                that refill idle lanes from the queue (ballot + one atomic
 //                per warp); hits are appended to the next shade queue.
-//   k_ctrl     - advances the queue counters (device-resident; the host
-//                never reads stage sizes).
+//   k_ctrl     - advances queue counters and path cursors and grants the
+//                free wavefront capacity to the active jobs in priority
+//                order (the host never reads stage sizes).
 //   k_resolve  - fixed-point accumulators -> get_image's tone map.
 // Every random number is drawn from a stream keyed by (job, ray, sample,
-// bounce) and radiance is summed in 2^-32 fixed point, so the image does not
-// depend on how paths are scheduled or batched.
+// bounce) and radiance is summed in 2^-32 fixed point, so a job's image does
+// not depend on how its paths are scheduled, batched or interleaved.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <numeric>
 
 #include "engine.h"
 #include "shading.cuh"
@@ -40,22 +46,29 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 
 struct EngineParams {
   DevJob* jobs;
-  int num_jobs;
+  DevSlot* slots;
+  int num_slots;
   DevCtrl* ctrl;
+  const int32_t* order;
+  int32_t* quota_slot;
+  int32_t* quota_prefix;
+  const int32_t* prim_slot;
+  const int64_t* prim_prefix;
+  int prim_n;
   float4* A_o[2];
   float4* A_d[2];
   float4* A_s[2];
   float4* A_r[2];
   int32_t* A_tri[2];
+  int32_t* A_leaf[2];   // leaf node of the hit (start hint for the next ray)
   float4* R_o;
   float4* R_d;
   float4* R_s;
   float4* R_r;
   int capacity;
-  int smem_nodes;   // > 0 only when every job uses shared_nodes' scene
+  int smem_nodes;       // > 0 only when every job uses shared_nodes' scene
   int refill;
   const DevNode* shared_nodes;
-  int64_t total_primary;
 };
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -64,23 +77,18 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   return m;
 }
 
-__device__ __forceinline__ int find_job_prim(const DevJob* jobs, int n, int64_t g) {
+// Index of the last prefix entry <= g (prefix[0] = 0, n entries).
+template <typename T>
+__device__ __forceinline__ int find_prefix(const T* prefix, int n, int64_t g) {
   int lo = 0, hi = n - 1;
   while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (jobs[mid].prim_base <= g) lo = mid; else hi = mid - 1;
+    const int mid = (lo + hi + 1) >> 1;
+    if ((int64_t)prefix[mid] <= g) lo = mid; else hi = mid - 1;
   }
   return lo;
 }
 
-__device__ __forceinline__ int find_job_path(const DevJob* jobs, int n, int64_t q) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (jobs[mid].path_base <= q) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
+__device__ __forceinline__ int64_t job_rays(const DevJob& J) { return (int64_t)J.nx * J.ny; }
 
 // Adds a path's radiance to its ray's fixed-point accumulator. Non-finite
 // or out-of-range values set a marker so the resolve reproduces the float
@@ -95,10 +103,19 @@ __device__ __forceinline__ void flush_radiance(const DevJob& J, int64_t ray, f3 
     } else if (!(fabsf(v[c]) < 1073741824.0f)) {
       atomicOr(J.flags + ray, 1u << (4 * c + (v[c] > 0.f ? 1 : 2)));
     } else {
-      long long q = __double2ll_rn((double)v[c] * kAccumScale);
+      const long long q = __double2ll_rn((double)v[c] * kAccumScale);
       atomicAdd(J.accum + 3 * ray + c, (unsigned long long)q);
     }
   }
+}
+
+// Counts finished paths per slot with one atomic per (warp, slot).
+__device__ __forceinline__ void count_done(DevSlot* slots, bool done, int slot) {
+  const unsigned m = __ballot_sync(kFull, done);
+  if (!m) return;
+  const unsigned same = __match_any_sync(kFull, done ? slot : -1);
+  if (done && (__ffs(same & m) - 1) == (int)(threadIdx.x & 31))
+    atomicAdd(&slots[slot].done, (unsigned long long)__popc(same & m));
 }
 
 // Warp-level reduction of the per-lane query and work counters.
@@ -108,12 +125,14 @@ __device__ __forceinline__ void flush_counts(DevCtrl* c, unsigned long long q, T
     n.nodes += __shfl_down_sync(kFull, n.nodes, o);
     n.leaves += __shfl_down_sync(kFull, n.leaves, o);
     n.tris += __shfl_down_sync(kFull, n.tris, o);
+    n.repeats += __shfl_down_sync(kFull, n.repeats, o);
   }
   if ((threadIdx.x & 31) == 0 && q) {
     atomicAdd(&c->isect_queries, q);
     atomicAdd(&c->nodes_visited, n.nodes);
     atomicAdd(&c->leaves_visited, n.leaves);
     atomicAdd(&c->tri_tests, n.tris);
+    atomicAdd(&c->tri_repeats, n.repeats);
   }
 }
 
@@ -125,57 +144,101 @@ __device__ __forceinline__ int stage_nodes(const EngineParams& P, uint2* snodes)
   return P.smem_nodes;
 }
 
+// Grants the free wavefront capacity to active slots in priority order
+// (one thread). A slot with nothing left to issue no longer needs grants.
+__device__ void schedule(const EngineParams& P) {
+  DevCtrl* c = P.ctrl;
+  const int budget = P.capacity - c->nA;
+  int n_new = 0, nq = 0;
+  bool remaining = false;
+  for (int k = 0; k < c->n_order; ++k) {
+    const int s = P.order[k];
+    HPT_DCHECK(&c->err, s >= 0 && s < P.num_slots, 231, s, continue);
+    DevSlot& S = P.slots[s];
+    S.alloc = 0;
+    if (!S.active) continue;
+    const int64_t rem = S.num_paths - S.cursor;
+    if (rem <= 0) continue;
+    remaining = true;
+    const int a = (int)min(rem, (int64_t)(budget - n_new));
+    if (a <= 0) continue;
+    S.alloc = a;
+    P.quota_slot[nq] = s;
+    P.quota_prefix[nq] = n_new;
+    n_new += a;
+    ++nq;
+  }
+  P.quota_prefix[nq] = n_new;
+  c->n_quota = nq;
+  c->n_new = n_new;
+  c->done = (c->nA == 0 && !remaining) ? 1 : 0;
+}
+
 // ---------------------------------------------------------------------------
 // Primary pass: raygen + closest hit, lanes refilled from a global counter.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_primary(EngineParams P) {
+template <int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
   extern __shared__ uint2 snodes[];
   const int n_smem = stage_nodes(P, snodes);
   DevCtrl* c = P.ctrl;
   const int lane = threadIdx.x & 31;
+  const int64_t total = P.prim_prefix[P.prim_n];
   bool active = false;
   TravState st;
-  int job = 0;
+  int slot = 0;
   int64_t ray = 0;
   unsigned long long queries = 0;
   TravCount cnt;
   while (true) {
     const unsigned idle = __ballot_sync(kFull, !active);
     if (__popc(idle) >= P.refill) {
-      unsigned long long base = 0;
-      if (lane == 0) base = atomicAdd(reinterpret_cast<unsigned long long*>(&c->cursor), (unsigned long long)__popc(idle));
+      int base = 0;
+      if (lane == 0) base = atomicAdd(&c->prim_head, __popc(idle));
       base = __shfl_sync(kFull, base, 0);
       if (!active) {
         const int64_t g = (int64_t)base + __popc(idle & lanemask_lt());
-        if (g < P.total_primary) {
-          job = find_job_prim(P.jobs, P.num_jobs, g);
-          const DevJob& J = P.jobs[job];
-          ray = g - J.prim_base;
-          const int x = (int)(ray % J.nx), y = (int)(ray / J.nx);
-          const f3 d = J.pano ? pano_dir(x, y, J.vr_x_shift, J.ny)
-                              : pinhole_dir(J.top, J.right, J.width, J.height, x, y, J.nx, J.ny);
-          Ray r{mk(J.view_p[0], J.view_p[1], J.view_p[2]), d};
-          trav_init(J.scene, r, st);
-          active = true;
-          ++queries;
+        if (g < total) {
+          const int e = find_prefix(P.prim_prefix, P.prim_n, g);
+          slot = P.prim_slot[e];
+          ray = g - P.prim_prefix[e];
+          bool ok = true;
+          HPT_DCHECK(&c->err, slot >= 0 && slot < P.num_slots, 201, slot, ok = false);
+          HPT_DCHECK(&c->err, !ok || (ray >= 0 && ray < job_rays(P.jobs[slot])), 202, ray,
+                     ok = false);
+          if (ok) {
+            const DevJob& J = P.jobs[slot];
+            const int x = (int)(ray % J.nx), y = (int)(ray / J.nx);
+            const f3 d = J.pano ? pano_dir(x, y, J.vr_x_shift, J.ny)
+                                : pinhole_dir(J.top, J.right, J.width, J.height, x, y, J.nx, J.ny);
+            trav_init(J.scene, Ray{mk(J.view_p[0], J.view_p[1], J.view_p[2]), d}, st);
+            active = true;
+            ++queries;
+#ifdef HPT_DEVICE_CHECKS
+            atomicAdd(&c->chk_isect_done, 1);
+#endif
+          }
         }
       }
     }
     if (__ballot_sync(kFull, active) == 0) break;
     bool finished = false;
-    if (active) finished = trav_leaf(P.jobs[job].scene, st, snodes, n_smem, &c->error, cnt);
+    if (active) finished = trav_leaf(P.jobs[slot].scene, st, snodes, n_smem, &c->err, cnt);
     if (finished) {
-      const DevJob& J = P.jobs[job];
+      const DevJob& J = P.jobs[slot];
       if (st.best.rec >= 0) {
-        const int k = atomicAdd(J.prim_count, 1);
-        float4* dst = reinterpret_cast<float4*>(J.prim) + 2 * (size_t)k;
-        dst[0] = make_float4(st.ray.d.x, st.ray.d.y, st.ray.d.z, __int_as_float((int)ray));
-        dst[1] = make_float4(__int_as_float(st.best.tri), st.best.t, 0.f, 0.f);
+        int k = atomicAdd(J.prim_count, 1);
+        HPT_DCHECK(&c->err, k < job_rays(J), 203, k, k = -1);
+        if (k >= 0) {
+          float4* dst = reinterpret_cast<float4*>(J.prim) + 2 * (size_t)k;
+          dst[0] = make_float4(st.ray.d.x, st.ray.d.y, st.ray.d.z, __int_as_float((int)ray));
+          dst[1] = make_float4(__int_as_float(st.best.tri), st.best.t,
+                               __int_as_float(st.best_node), 0.f);
+        }
       } else {
         // kernel.cl:193-206: the first pass assigns background * strength *
         // sample_n with strength (1,1,1).
-        const float spp = (float)J.spp;
-        const f3 val = scale(spp, mul(mk(J.bg[0], J.bg[1], J.bg[2]), mk(1.f, 1.f, 1.f)));
+        const f3 val = scale((float)J.spp, mul(mk(J.bg[0], J.bg[1], J.bg[2]), mk(1.f, 1.f, 1.f)));
         flush_radiance(J, ray, val);
       }
       active = false;
@@ -184,24 +247,25 @@ __global__ void __launch_bounds__(256) k_primary(EngineParams P) {
   flush_counts(c, queries, cnt);
 }
 
-// Sets path ranges after the primary pass (one thread).
-__global__ void k_setup(DevJob* jobs, int n, DevCtrl* c) {
-  int64_t base = 0;
-  for (int j = 0; j < n; ++j) {
-    const int64_t np = (int64_t)(*jobs[j].prim_count) * jobs[j].spp;
-    jobs[j].path_base = base;
-    jobs[j].num_paths = np;
-    base += np;
+// Sets the path counts of newly admitted slots and grants paths (one thread).
+__global__ void k_admit(EngineParams P) {
+#ifdef HPT_DEVICE_CHECKS
+  HPT_DCHECK(&P.ctrl->err, P.ctrl->chk_isect_done == P.prim_prefix[P.prim_n], 243,
+             P.ctrl->chk_isect_done, (void)0);
+  P.ctrl->chk_isect_done = 0;
+#endif
+  for (int e = 0; e < P.prim_n; ++e) {
+    const int s = P.prim_slot[e];
+    HPT_DCHECK(&P.ctrl->err, s >= 0 && s < P.num_slots, 232, s, continue);
+    DevSlot& S = P.slots[s];
+    S.num_paths = (int64_t)(*P.jobs[s].prim_count) * P.jobs[s].spp;
+    S.cursor = 0;
+    S.done = 0;
+    S.alloc = 0;
+    S.active = 1;
   }
-  c->total_paths = base;
-  c->cursor = 0;
-  c->nA = 0;
-  c->nA_next = 0;
-  c->nR = 0;
-  c->isect_head = 0;
-  c->n_new = 0;
-  c->parity = 0;
-  c->done = base == 0 ? 1 : 0;
+  P.ctrl->prim_head = 0;
+  schedule(P);
 }
 
 // ---------------------------------------------------------------------------
@@ -214,74 +278,105 @@ __global__ void __launch_bounds__(BS) k_shade(EngineParams P) {
   DevCtrl* c = P.ctrl;
   const int par = c->parity;
   const int nA = c->nA;
-  const int64_t cursor = c->cursor, total = c->total_paths;
-  const int64_t room = (int64_t)P.capacity - nA;
-  const int n_new = (int)max((int64_t)0, min(room, total - cursor));
-  if (blockIdx.x == 0 && threadIdx.x == 0) c->n_new = n_new;
+  const int n_new = c->n_new, n_quota = c->n_quota;
   const int n_items = nA + n_new;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned long long shades = 0;
+#ifdef HPT_DEVICE_CHECKS
+  if (blockIdx.x == 0 && threadIdx.x == 0) c->chk_shade_items = n_items;
+  int chk_items = 0;
+#endif
   for (int base = blockIdx.x * BS; base < n_items; base += gridDim.x * BS) {
     const int i = base + threadIdx.x;
-    bool alive = false;
+#ifdef HPT_DEVICE_CHECKS
+    if (i < n_items) ++chk_items;
+#endif
+    bool alive = false, ended = false;
+    int slot = 0;
     float4 oo, dd, ss, rr;
     if (i < n_items) {
-      int job, sample, bounce, tri;
-      int64_t ray;
+      int sample = 0, bounce = 0, tri = -1, hint = -1;
+      int64_t ray = -1;
       f3 o, d, strength, rad;
-      float t;
+      float t = 0.f;
+      bool ok = true;
       if (i < nA) {
-        const float4 ao = P.A_o[par][i], ad = P.A_d[par][i], as = P.A_s[par][i], ar = P.A_r[par][i];
-        tri = P.A_tri[par][i];
-        o = mk(ao.x, ao.y, ao.z);
-        ray = __float_as_int(ao.w);
-        d = mk(ad.x, ad.y, ad.z);
-        const uint32_t meta = __float_as_uint(ad.w);
-        sample = (int)(meta >> 8);
-        bounce = (int)(meta & 0xFF);
-        strength = mk(as.x, as.y, as.z);
-        job = __float_as_int(as.w);
-        rad = mk(ar.x, ar.y, ar.z);
-        t = ar.w;
+        HPT_DCHECK(&c->err, i < P.capacity, 211, i, ok = false);
+        if (ok) {
+          const float4 ao = P.A_o[par][i], ad = P.A_d[par][i], as = P.A_s[par][i],
+                       ar = P.A_r[par][i];
+          tri = P.A_tri[par][i];
+          hint = P.A_leaf[par][i];
+          o = mk(ao.x, ao.y, ao.z);
+          ray = __float_as_int(ao.w);
+          d = mk(ad.x, ad.y, ad.z);
+          const uint32_t meta = __float_as_uint(ad.w);
+          sample = (int)(meta >> 8);
+          bounce = (int)(meta & 0xFF);
+          strength = mk(as.x, as.y, as.z);
+          slot = __float_as_int(as.w);
+          rad = mk(ar.x, ar.y, ar.z);
+          t = ar.w;
+        }
       } else {
-        const int64_t q = cursor + (i - nA);
-        job = find_job_path(P.jobs, P.num_jobs, q);
-        const DevJob& J = P.jobs[job];
-        const int64_t local = q - J.path_base;
-        const int nh = *J.prim_count;
-        const int64_t k = local % nh;
-        sample = (int)(local / nh);
-        bounce = 0;
-        const float4* src = reinterpret_cast<const float4*>(J.prim) + 2 * k;
-        const float4 p0 = src[0], p1 = src[1];
-        o = mk(J.view_p[0], J.view_p[1], J.view_p[2]);
-        d = mk(p0.x, p0.y, p0.z);
-        ray = __float_as_int(p0.w);
-        tri = __float_as_int(p1.x);
-        t = p1.y;
-        strength = mk(1.f, 1.f, 1.f);
-        rad = mk(0.f, 0.f, 0.f);
-      }
-      const DevJob& J = P.jobs[job];
-      uint64_t seed = path_seed(J.seed, (uint32_t)ray, (uint32_t)sample, (uint32_t)bounce);
-      const Ray r{o, d};
-      const ShadeOut so = shade_hit(J.scene, r, strength, tri, t, J.disable_diffuse, seed);
-      ++shades;
-      rad = add(rad, so.contrib);
-      if (so.branch != kDead && bounce + 1 < J.depth) {
-        const NextOut no = next_direction(J.scene, so.branch, d, so.hit_p, so.normal,
-                                          so.strength, so.param, seed);
-        if (no.alive) {
-          alive = true;
-          oo = make_float4(no.o.x, no.o.y, no.o.z, __int_as_float((int)ray));
-          dd = make_float4(no.d.x, no.d.y, no.d.z,
-                           __uint_as_float(((uint32_t)sample << 8) | (uint32_t)(bounce + 1)));
-          ss = make_float4(no.strength.x, no.strength.y, no.strength.z, __int_as_float(job));
-          rr = make_float4(rad.x, rad.y, rad.z, 0.f);
+        const int off = i - nA;
+        const int e = find_prefix(P.quota_prefix, n_quota, off);
+        slot = P.quota_slot[e];
+        HPT_DCHECK(&c->err, slot >= 0 && slot < P.num_slots, 212, slot, ok = false);
+        if (ok) {
+          const DevJob& J = P.jobs[slot];
+          const int64_t q = P.slots[slot].cursor + (off - P.quota_prefix[e]);
+          const int nh = *J.prim_count;
+          HPT_DCHECK(&c->err, nh > 0 && q < (int64_t)nh * J.spp, 213, q, ok = false);
+          HPT_DCHECK(&c->err, !ok || nh <= job_rays(J), 217, nh, ok = false);
+          if (ok) {
+            const int64_t k = q % nh;
+            sample = (int)(q / nh);
+            bounce = 0;
+            const float4* src = reinterpret_cast<const float4*>(J.prim) + 2 * k;
+            const float4 p0 = src[0], p1 = src[1];
+            o = mk(J.view_p[0], J.view_p[1], J.view_p[2]);
+            d = mk(p0.x, p0.y, p0.z);
+            ray = __float_as_int(p0.w);
+            tri = __float_as_int(p1.x);
+            t = p1.y;
+            hint = __float_as_int(p1.z);
+            strength = mk(1.f, 1.f, 1.f);
+            rad = mk(0.f, 0.f, 0.f);
+          }
         }
       }
-      if (!alive) flush_radiance(J, ray, rad);
+      HPT_DCHECK(&c->err, !ok || (slot >= 0 && slot < P.num_slots), 212, slot, ok = false);
+      HPT_DCHECK(&c->err, !ok || (tri >= 0 && tri < P.jobs[slot].scene.num_triangles), 214, tri,
+                 ok = false);
+      HPT_DCHECK(&c->err, !ok || (ray >= 0 && ray < job_rays(P.jobs[slot])), 215, ray, ok = false);
+      if (ok) {
+        const DevJob& J = P.jobs[slot];
+        uint64_t seed = path_seed(J.seed, (uint32_t)ray, (uint32_t)sample, (uint32_t)bounce);
+        const Ray r{o, d};
+        const ShadeOut so = shade_hit(J.scene, r, strength, tri, t, J.disable_diffuse, seed,
+                                      &c->err);
+        ++shades;
+        rad = add(rad, so.contrib);
+        if (so.branch != kDead && bounce + 1 < J.depth) {
+          const NextOut no = next_direction(J.scene, so.branch, d, so.hit_p, so.normal,
+                                            so.strength, so.param, seed, &c->err);
+          if (no.alive) {
+            alive = true;
+            oo = make_float4(no.o.x, no.o.y, no.o.z, __int_as_float((int)ray));
+            dd = make_float4(no.d.x, no.d.y, no.d.z,
+                             __uint_as_float(((uint32_t)sample << 8) | (uint32_t)(bounce + 1)));
+            ss = make_float4(no.strength.x, no.strength.y, no.strength.z, __int_as_float(slot));
+            rr = make_float4(rad.x, rad.y, rad.z, __int_as_float(hint));
+          }
+        }
+        if (!alive) {
+          flush_radiance(J, ray, rad);
+          ended = true;
+        }
+      }
     }
+    count_done(P.slots, ended, slot);
     // Block-level stable compaction: ballot per warp, scan over warps.
     const unsigned m = __ballot_sync(kFull, alive);
     if (lane == 0) warp_counts[warp] = __popc(m);
@@ -298,21 +393,30 @@ __global__ void __launch_bounds__(BS) k_shade(EngineParams P) {
     __syncthreads();
     if (alive) {
       const int pos = block_base + warp_counts[warp] + __popc(m & lanemask_lt());
-      P.R_o[pos] = oo;
-      P.R_d[pos] = dd;
-      P.R_s[pos] = ss;
-      P.R_r[pos] = rr;
+      bool ok = true;
+      HPT_DCHECK(&c->err, pos < P.capacity, 216, pos, ok = false);
+      if (ok) {
+        P.R_o[pos] = oo;
+        P.R_d[pos] = dd;
+        P.R_s[pos] = ss;
+        P.R_r[pos] = rr;
+      }
     }
     __syncthreads();
   }
   for (int o = 16; o > 0; o >>= 1) shades += __shfl_down_sync(kFull, shades, o);
   if (lane == 0 && shades) atomicAdd(&c->shades, shades);
+#ifdef HPT_DEVICE_CHECKS
+  for (int o = 16; o > 0; o >>= 1) chk_items += __shfl_down_sync(kFull, chk_items, o);
+  if (lane == 0 && chk_items) atomicAdd(&c->chk_shade_done, chk_items);
+#endif
 }
 
 // ---------------------------------------------------------------------------
 // Intersect queue -> next shade queue, persistent warps with lane refill.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_isect(EngineParams P) {
+template <int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
   extern __shared__ uint2 snodes[];
   const int n_smem = stage_nodes(P, snodes);
   DevCtrl* c = P.ctrl;
@@ -321,9 +425,8 @@ __global__ void __launch_bounds__(256) k_isect(EngineParams P) {
   const int lane = threadIdx.x & 31;
   bool active = false;
   TravState st;
-  float4 s4 = make_float4(0, 0, 0, 0), r4 = make_float4(0, 0, 0, 0);
-  float ow = 0.f, dw = 0.f;
-  int job = 0;
+  int item = 0;   // index in the intersect queue; the payload is reloaded at the end
+  int slot = 0;
   unsigned long long queries = 0;
   TravCount cnt;
   while (true) {
@@ -335,21 +438,29 @@ __global__ void __launch_bounds__(256) k_isect(EngineParams P) {
       if (!active) {
         const int i = base + __popc(idle & lanemask_lt());
         if (i < n) {
-          const float4 o4 = P.R_o[i], d4 = P.R_d[i];
-          s4 = P.R_s[i];
-          r4 = P.R_r[i];
-          ow = o4.w;
-          dw = d4.w;
-          job = __float_as_int(s4.w);
-          trav_init(P.jobs[job].scene, Ray{mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z)}, st);
-          active = true;
-          ++queries;
+          bool ok = true;
+          HPT_DCHECK(&c->err, i < P.capacity, 221, i, ok = false);
+          if (ok) {
+            const float4 o4 = P.R_o[i], d4 = P.R_d[i];
+            item = i;
+            slot = __float_as_int(P.R_s[i].w);
+            HPT_DCHECK(&c->err, slot >= 0 && slot < P.num_slots, 222, slot, ok = false);
+            if (ok) {
+              trav_init(P.jobs[slot].scene, Ray{mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z)}, st,
+                        __float_as_int(P.R_r[i].w));
+              active = true;
+              ++queries;
+#ifdef HPT_DEVICE_CHECKS
+              atomicAdd(&c->chk_isect_done, 1);
+#endif
+            }
+          }
         }
       }
     }
     if (__ballot_sync(kFull, active) == 0) break;
     bool finished = false;
-    if (active) finished = trav_leaf(P.jobs[job].scene, st, snodes, n_smem, &c->error, cnt);
+    if (active) finished = trav_leaf(P.jobs[slot].scene, st, snodes, n_smem, &c->err, cnt);
     const bool hit = finished && st.best.rec >= 0;
     const unsigned hm = __ballot_sync(kFull, hit);
     if (hm) {
@@ -359,36 +470,81 @@ __global__ void __launch_bounds__(256) k_isect(EngineParams P) {
       base = __shfl_sync(kFull, base, leader);
       if (hit) {
         const int pos = base + __popc(hm & lanemask_lt());
-        P.A_o[out_par][pos] = make_float4(st.ray.o.x, st.ray.o.y, st.ray.o.z, ow);
-        P.A_d[out_par][pos] = make_float4(st.ray.d.x, st.ray.d.y, st.ray.d.z, dw);
-        P.A_s[out_par][pos] = s4;
-        P.A_r[out_par][pos] = make_float4(r4.x, r4.y, r4.z, st.best.t);
-        P.A_tri[out_par][pos] = st.best.tri;
+        bool ok = true;
+        HPT_DCHECK(&c->err, pos < P.capacity, 223, pos, ok = false);
+        if (ok) {
+          const float4 r4 = P.R_r[item];
+          P.A_o[out_par][pos] = P.R_o[item];
+          P.A_d[out_par][pos] = P.R_d[item];
+          P.A_s[out_par][pos] = P.R_s[item];
+          P.A_r[out_par][pos] = make_float4(r4.x, r4.y, r4.z, st.best.t);
+          P.A_tri[out_par][pos] = st.best.tri;
+          P.A_leaf[out_par][pos] = st.best_node;
+        }
       }
     }
-    if (finished && !hit) {
+    const bool missed = finished && !hit;
+    if (missed) {
       // kernel.cl:195-200: miss adds background * strength (sample_n = 1).
-      const DevJob& J = P.jobs[job];
-      f3 rad = mk(r4.x, r4.y, r4.z);
-      rad = add(rad, mul(mk(J.bg[0], J.bg[1], J.bg[2]), mk(s4.x, s4.y, s4.z)));
-      flush_radiance(J, __float_as_int(ow), rad);
+      const DevJob& J = P.jobs[slot];
+      const float4 s4 = P.R_s[item], r4 = P.R_r[item];
+      const int64_t ray = __float_as_int(P.R_o[item].w);
+      bool ok = true;
+      HPT_DCHECK(&c->err, ray >= 0 && ray < job_rays(J), 224, ray, ok = false);
+      if (ok) {
+        f3 rad = mk(r4.x, r4.y, r4.z);
+        rad = add(rad, mul(mk(J.bg[0], J.bg[1], J.bg[2]), mk(s4.x, s4.y, s4.z)));
+        flush_radiance(J, ray, rad);
+      }
     }
+    count_done(P.slots, missed, slot);
     if (finished) active = false;
   }
   flush_counts(c, queries, cnt);
 }
 
-__global__ void k_ctrl(DevCtrl* c) {
+// Advances the queues and the path cursors, then grants paths (one thread).
+__global__ void k_ctrl(EngineParams P) {
+  DevCtrl* c = P.ctrl;
+#ifdef HPT_DEVICE_CHECKS
+  HPT_DCHECK(&c->err, c->chk_shade_done == c->chk_shade_items, 241,
+             (long long)c->chk_shade_items * 1000000 + c->chk_shade_done, (void)0);
+  HPT_DCHECK(&c->err, c->chk_isect_done == c->nR, 242,
+             (long long)c->nR * 1000000 + c->chk_isect_done, (void)0);
+  c->chk_shade_items = 0;
+  c->chk_shade_done = 0;
+  c->chk_isect_done = 0;
+#endif
+  for (int k = 0; k < c->n_quota; ++k) {
+    DevSlot& S = P.slots[P.quota_slot[k]];
+    S.cursor += S.alloc;
+    S.alloc = 0;
+  }
   c->nA = c->nA_next;
   c->nA_next = 0;
   c->nR = 0;
   c->isect_head = 0;
-  c->cursor += c->n_new;
-  c->n_new = 0;
   c->parity ^= 1;
   c->iterations += 1;
-  c->done = (c->nA == 0 && c->cursor >= c->total_paths) ? 1 : 0;
+  schedule(P);
 }
+
+// Register budgets for the traversal kernels: (threads per block, blocks
+// per SM the compiler must fit). The natural allocation is ~97 registers;
+// tighter budgets trade spills for resident warps. Chosen by the tuning.
+struct IsectVariant {
+  int block, min_blocks;
+  void (*isect)(EngineParams);
+  void (*primary)(EngineParams);
+};
+const IsectVariant kIsectVariants[] = {
+    {128, 5, k_isect<128, 5>, k_primary<128, 5>},
+    {128, 6, k_isect<128, 6>, k_primary<128, 6>},
+    {128, 8, k_isect<128, 8>, k_primary<128, 8>},
+    {256, 2, k_isect<256, 2>, k_primary<256, 2>},
+    {256, 3, k_isect<256, 3>, k_primary<256, 3>},
+};
+constexpr int kNumIsectVariants = sizeof(kIsectVariants) / sizeof(kIsectVariants[0]);
 
 __device__ __forceinline__ float ray_value(const unsigned long long* acc, const uint32_t* flags,
                                            int64_t ray, int ch) {
@@ -409,9 +565,11 @@ __device__ __forceinline__ uint8_t to_unorm8(float x) {
   return (uint8_t)__float2int_rn(v);
 }
 
-// get_image (kernel.cl:615-652) from the fixed-point accumulators.
-__global__ void k_resolve(const DevJob* jp, int W, int H, int ssx, int ssy, float brightness,
-                          uint8_t* rgba, float* accum_f) {
+// get_image (kernel.cl:615-652) from the fixed-point accumulators. spp is
+// the divisor (the full sample count, or the samples completed so far for a
+// progressive preview).
+__global__ void k_resolve(const DevJob* jp, int W, int H, int ssx, int ssy, int spp,
+                          float brightness, uint8_t* rgba, float* accum_f) {
   const int gx = blockIdx.x * blockDim.x + threadIdx.x;
   const int gy = blockIdx.y * blockDim.y + threadIdx.y;
   if (gx >= W || gy >= H) return;
@@ -433,7 +591,7 @@ __global__ void k_resolve(const DevJob* jp, int W, int H, int ssx, int ssy, floa
       py = __fadd_rn(py, vy);
       pz = __fadd_rn(pz, vz);
     }
-  const float nss = (float)(ssx * ssy), ns = (float)J.spp;
+  const float nss = (float)(ssx * ssy), ns = (float)spp;
   px = __fmul_rn(__fdiv_rn(__fdiv_rn(px, nss), ns), brightness);
   py = __fmul_rn(__fdiv_rn(__fdiv_rn(py, nss), ns), brightness);
   pz = __fmul_rn(__fdiv_rn(__fdiv_rn(pz, nss), ns), brightness);
@@ -455,11 +613,22 @@ hpt_status cuda_fail(cudaError_t e, const char* what) {
               what, cudaGetErrorString(e));
 }
 
+void cuda_soft_fail(cudaError_t e, const char* what) {
+  (void)cudaGetLastError();
+#ifdef HPT_DEVICE_CHECKS
+  fprintf(stderr, "hpt: best-effort call failed: %s: %s\n", what, cudaGetErrorString(e));
+#else
+  (void)e;
+  (void)what;
+#endif
+}
+
 hpt_tuning default_tuning() {
   hpt_tuning t;
   memset(&t, 0, sizeof t);
   t.capacity = 1 << 21;
-  t.isect_block = 256;
+  t.isect_block = 128;
+  t.isect_min_blocks = 5;
   t.shade_block = 256;
   t.refill_chunk = 16;
   t.smem_nodes = 2048;
@@ -467,39 +636,93 @@ hpt_tuning default_tuning() {
   return t;
 }
 
+hpt_status check_render_params(const hpt_camera* cam, const hpt_render_params* p) {
+  if (!cam || !p) return fail(HPT_ERR_INVALID_ARGUMENT, "camera/params is NULL");
+  if (p->sample_x <= 0 || p->sample_y <= 0 || p->supersample_x <= 0 || p->supersample_y <= 0 ||
+      p->sample <= 0 || p->depth <= 0)
+    return fail(HPT_ERR_INVALID_ARGUMENT, "sizes, sample and depth must be positive");
+  const int64_t rays = (int64_t)p->sample_x * p->supersample_x * p->sample_y * p->supersample_y;
+  if (rays > (1ll << 30)) return fail(HPT_ERR_INVALID_ARGUMENT, "too many rays per frame");
+  if (p->sample >= (1 << 24)) return fail(HPT_ERR_INVALID_ARGUMENT, "sample must be < 2^24");
+  if (p->depth > 255) return fail(HPT_ERR_INVALID_ARGUMENT, "depth must be <= 255");
+  if (cam->height < 0 && p->supersample_x != p->supersample_y)
+    return fail(HPT_ERR_INVALID_ARGUMENT,
+                "panorama needs supersample_x == supersample_y (the reference indexes rays with "
+                "sample_x * supersample_y)");
+  return HPT_OK;
+}
+
+int64_t job_footprint(const hpt_render_params& p, bool want_accum) {
+  const int64_t rays = (int64_t)p.sample_x * p.supersample_x * p.sample_y * p.supersample_y;
+  return rays * (24 + 4 + 32 + (want_accum ? 12 : 0)) + (int64_t)p.sample_x * p.sample_y * 4 + 64;
+}
+
 Engine::Engine(int dev) : device(dev) {
   tuning = default_tuning();
-  cudaSetDevice(device);
-  cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
-  cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device);
-  cudaMalloc(&ctrl_, sizeof(DevCtrl));
-  cudaMallocHost(&ctrl_host_, sizeof(DevCtrl));
-  for (auto& e : ev_) cudaEventCreate(&e);
+  for (auto& e : ev_) e = nullptr;
+  init_status_ = init();
+}
+
+// Device resources every run needs; a failure is reported by run().
+hpt_status Engine::init() {
+  HPT_CUDA(cudaSetDevice(device));
+  HPT_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  HPT_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+  HPT_CUDA(cudaMalloc(&ctrl_, sizeof(DevCtrl)));
+  HPT_CUDA(cudaMallocHost(&ctrl_host_, sizeof(DevCtrl)));
+  for (auto& e : ev_) HPT_CUDA(cudaEventCreate(&e));
+  return HPT_OK;
 }
 
 Engine::~Engine() {
-  cudaSetDevice(device);
-  if (stream) cudaStreamSynchronize(stream);
+  HPT_SOFT(cudaSetDevice(device));
+  if (stream) HPT_SOFT(cudaStreamSynchronize(stream));
   for (int p = 0; p < 2; ++p) {
-    cudaFree(A_o_[p]); cudaFree(A_d_[p]); cudaFree(A_s_[p]); cudaFree(A_r_[p]); cudaFree(A_tri_[p]);
+    HPT_SOFT(cudaFree(A_o_[p]));
+    HPT_SOFT(cudaFree(A_d_[p]));
+    HPT_SOFT(cudaFree(A_s_[p]));
+    HPT_SOFT(cudaFree(A_r_[p]));
+    HPT_SOFT(cudaFree(A_tri_[p]));
+    HPT_SOFT(cudaFree(A_leaf_[p]));
   }
-  cudaFree(R_o_); cudaFree(R_d_); cudaFree(R_s_); cudaFree(R_r_);
-  cudaFree(ctrl_);
-  cudaFree(jobs_);
-  cudaFreeHost(ctrl_host_);
-  for (auto& e : ev_) cudaEventDestroy(e);
-  if (stream) cudaStreamDestroy(stream);
+  HPT_SOFT(cudaFree(R_o_));
+  HPT_SOFT(cudaFree(R_d_));
+  HPT_SOFT(cudaFree(R_s_));
+  HPT_SOFT(cudaFree(R_r_));
+  HPT_SOFT(cudaFree(ctrl_));
+  HPT_SOFT(cudaFree(jobs_));
+  HPT_SOFT(cudaFree(slot_state_));
+  HPT_SOFT(cudaFree(order_));
+  HPT_SOFT(cudaFree(quota_slot_));
+  HPT_SOFT(cudaFree(quota_prefix_));
+  HPT_SOFT(cudaFree(prim_slot_));
+  HPT_SOFT(cudaFree(prim_prefix_));
+  HPT_SOFT(cudaFreeHost(ctrl_host_));
+  HPT_SOFT(cudaFreeHost(host_i32_));
+  HPT_SOFT(cudaFreeHost(host_i64_));
+  HPT_SOFT(cudaFreeHost(host_jobs_));
+  for (auto& e : ev_)
+    if (e) HPT_SOFT(cudaEventDestroy(e));
+  if (stream) HPT_SOFT(cudaStreamDestroy(stream));
 }
 
 hpt_status Engine::ensure_capacity(int capacity) {
   if (capacity <= capacity_) return HPT_OK;
-  cudaStreamSynchronize(stream);
+  HPT_SOFT(cudaStreamSynchronize(stream));
   for (int p = 0; p < 2; ++p) {
-    cudaFree(A_o_[p]); cudaFree(A_d_[p]); cudaFree(A_s_[p]); cudaFree(A_r_[p]); cudaFree(A_tri_[p]);
+    HPT_SOFT(cudaFree(A_o_[p]));
+    HPT_SOFT(cudaFree(A_d_[p]));
+    HPT_SOFT(cudaFree(A_s_[p]));
+    HPT_SOFT(cudaFree(A_r_[p]));
+    HPT_SOFT(cudaFree(A_tri_[p]));
+    HPT_SOFT(cudaFree(A_leaf_[p]));
     A_o_[p] = A_d_[p] = A_s_[p] = A_r_[p] = nullptr;
-    A_tri_[p] = nullptr;
+    A_tri_[p] = A_leaf_[p] = nullptr;
   }
-  cudaFree(R_o_); cudaFree(R_d_); cudaFree(R_s_); cudaFree(R_r_);
+  HPT_SOFT(cudaFree(R_o_));
+  HPT_SOFT(cudaFree(R_d_));
+  HPT_SOFT(cudaFree(R_s_));
+  HPT_SOFT(cudaFree(R_r_));
   R_o_ = R_d_ = R_s_ = R_r_ = nullptr;
   capacity_ = 0;
   const size_t n = (size_t)capacity;
@@ -509,6 +732,7 @@ hpt_status Engine::ensure_capacity(int capacity) {
     HPT_CUDA(cudaMalloc(&A_s_[p], n * sizeof(float4)));
     HPT_CUDA(cudaMalloc(&A_r_[p], n * sizeof(float4)));
     HPT_CUDA(cudaMalloc(&A_tri_[p], n * sizeof(int32_t)));
+    HPT_CUDA(cudaMalloc(&A_leaf_[p], n * sizeof(int32_t)));
   }
   HPT_CUDA(cudaMalloc(&R_o_, n * sizeof(float4)));
   HPT_CUDA(cudaMalloc(&R_d_, n * sizeof(float4)));
@@ -518,15 +742,89 @@ hpt_status Engine::ensure_capacity(int capacity) {
   return HPT_OK;
 }
 
-void Engine::query_occupancy() {
-  if (occ_done_) return;
+hpt_status Engine::ensure_slots(int slots) {
+  if (slots <= slots_) return HPT_OK;
+  HPT_SOFT(cudaStreamSynchronize(stream));
+  HPT_SOFT(cudaFree(jobs_));
+  HPT_SOFT(cudaFree(slot_state_));
+  HPT_SOFT(cudaFree(order_));
+  HPT_SOFT(cudaFree(quota_slot_));
+  HPT_SOFT(cudaFree(quota_prefix_));
+  HPT_SOFT(cudaFree(prim_slot_));
+  HPT_SOFT(cudaFree(prim_prefix_));
+  HPT_SOFT(cudaFreeHost(host_i32_));
+  HPT_SOFT(cudaFreeHost(host_i64_));
+  HPT_SOFT(cudaFreeHost(host_jobs_));
+  jobs_ = nullptr;
+  slot_state_ = nullptr;
+  order_ = quota_slot_ = quota_prefix_ = prim_slot_ = nullptr;
+  prim_prefix_ = nullptr;
+  host_i32_ = nullptr;
+  host_i64_ = nullptr;
+  host_jobs_ = nullptr;
+  slots_ = 0;
+  const size_t n = (size_t)slots;
+  HPT_CUDA(cudaMalloc(&jobs_, n * sizeof(DevJob)));
+  HPT_CUDA(cudaMalloc(&slot_state_, n * sizeof(DevSlot)));
+  HPT_CUDA(cudaMalloc(&order_, n * sizeof(int32_t)));
+  HPT_CUDA(cudaMalloc(&quota_slot_, n * sizeof(int32_t)));
+  HPT_CUDA(cudaMalloc(&quota_prefix_, (n + 1) * sizeof(int32_t)));
+  HPT_CUDA(cudaMalloc(&prim_slot_, n * sizeof(int32_t)));
+  HPT_CUDA(cudaMalloc(&prim_prefix_, (n + 1) * sizeof(int64_t)));
+  HPT_CUDA(cudaMallocHost(&host_i32_, (2 * n + 3) * sizeof(int32_t)));
+  HPT_CUDA(cudaMallocHost(&host_i64_, (n + 1) * sizeof(int64_t)));
+  HPT_CUDA(cudaMallocHost(&host_jobs_, n * sizeof(DevJob)));
+  HPT_CUDA(cudaMemsetAsync(jobs_, 0, n * sizeof(DevJob), stream));
+  HPT_CUDA(cudaMemsetAsync(slot_state_, 0, n * sizeof(DevSlot), stream));
+  HPT_CUDA(cudaMemsetAsync(quota_prefix_, 0, (n + 1) * sizeof(int32_t), stream));
+  HPT_CUDA(cudaMemsetAsync(prim_prefix_, 0, (n + 1) * sizeof(int64_t), stream));
+  slots_ = slots;
+  return HPT_OK;
+}
+
+// The compiled variant with the tuning's block size and blocks-per-SM
+// budget; without an exact match, the first one with that block size.
+int Engine::isect_variant() const {
+  for (int i = 0; i < kNumIsectVariants; ++i)
+    if (kIsectVariants[i].block == tuning.isect_block &&
+        kIsectVariants[i].min_blocks == tuning.isect_min_blocks)
+      return i;
+  for (int i = 0; i < kNumIsectVariants; ++i)
+    if (kIsectVariants[i].block == tuning.isect_block) return i;
+  return 0;
+}
+
+// The dynamic shared-memory limit is an attribute of the kernel function
+// (per device, shared by every engine of the process), so it is raised once
+// to the largest node prefix a tuning may ask for and never lowered.
+static hpt_status raise_smem_limits(int device) {
+  static std::mutex mu;
+  static std::vector<char> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)done.size() <= device) done.resize(device + 1, 0);
+  if (done[device]) return HPT_OK;
+  const int bytes = kMaxSmemNodes * (int)sizeof(uint2);
+  for (const IsectVariant& v : kIsectVariants) {
+    HPT_CUDA(cudaFuncSetAttribute(v.primary, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    HPT_CUDA(cudaFuncSetAttribute(v.isect, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  }
+  done[device] = 1;
+  return HPT_OK;
+}
+
+hpt_status Engine::query_occupancy() {
+  if (occ_done_) return HPT_OK;
+  hpt_status s = raise_smem_limits(device);
+  if (s != HPT_OK) return s;
+  const IsectVariant& v = kIsectVariants[isect_variant()];
   const size_t smem = (size_t)std::max(0, tuning.smem_nodes) * sizeof(uint2);
   int b = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_isect, 256, smem);
+  HPT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, v.isect, v.block, smem));
   occ_isect_ = std::max(1, b);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<256>, 256, 0);
+  HPT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<256>, 256, 0));
   occ_shade_ = std::max(1, b);
   occ_done_ = true;
+  return HPT_OK;
 }
 
 hpt_status Engine::alloc_job(const JobSpec& js, bool want_accum, JobBuffers& b) {
@@ -537,29 +835,26 @@ hpt_status Engine::alloc_job(const JobSpec& js, bool want_accum, JobBuffers& b) 
   HPT_CUDA(cudaMallocAsync(&b.flags, (size_t)b.rays * sizeof(uint32_t), stream));
   HPT_CUDA(cudaMallocAsync(&b.prim, (size_t)b.rays * 8 * sizeof(float), stream));
   HPT_CUDA(cudaMallocAsync(&b.prim_count, sizeof(int32_t), stream));
-  HPT_CUDA(cudaMallocAsync(&b.counters, 4 * sizeof(unsigned long long), stream));
   HPT_CUDA(cudaMallocAsync(&b.rgba, (size_t)p.sample_x * p.sample_y * 4, stream));
   if (want_accum) HPT_CUDA(cudaMallocAsync(&b.accum_f, (size_t)b.rays * 3 * sizeof(float), stream));
   HPT_CUDA(cudaMemsetAsync(b.accum, 0, (size_t)b.rays * 3 * sizeof(unsigned long long), stream));
   HPT_CUDA(cudaMemsetAsync(b.flags, 0, (size_t)b.rays * sizeof(uint32_t), stream));
   HPT_CUDA(cudaMemsetAsync(b.prim_count, 0, sizeof(int32_t), stream));
-  HPT_CUDA(cudaMemsetAsync(b.counters, 0, 4 * sizeof(unsigned long long), stream));
-  b.bytes = b.rays * (24 + 4 + 32 + (want_accum ? 12 : 0)) + (int64_t)p.sample_x * p.sample_y * 4;
+  b.bytes = job_footprint(p, want_accum);
   return HPT_OK;
 }
 
 void Engine::free_job(JobBuffers& b) {
-  cudaFreeAsync(b.accum, stream);
-  cudaFreeAsync(b.flags, stream);
-  cudaFreeAsync(b.prim, stream);
-  cudaFreeAsync(b.prim_count, stream);
-  cudaFreeAsync(b.counters, stream);
-  cudaFreeAsync(b.rgba, stream);
-  if (b.accum_f) cudaFreeAsync(b.accum_f, stream);
+  HPT_SOFT(cudaFreeAsync(b.accum, stream));
+  HPT_SOFT(cudaFreeAsync(b.flags, stream));
+  HPT_SOFT(cudaFreeAsync(b.prim, stream));
+  HPT_SOFT(cudaFreeAsync(b.prim_count, stream));
+  HPT_SOFT(cudaFreeAsync(b.rgba, stream));
+  if (b.accum_f) HPT_SOFT(cudaFreeAsync(b.accum_f, stream));
   b = JobBuffers();
 }
 
-DevJob Engine::make_job(const JobSpec& js, const JobBuffers& b, int64_t prim_base) const {
+DevJob Engine::make_job(const JobSpec& js, const JobBuffers& b) const {
   DevJob j;
   memset(&j, 0, sizeof j);
   const hpt_camera& cam = js.camera;
@@ -578,8 +873,6 @@ DevJob Engine::make_job(const JobSpec& js, const JobBuffers& b, int64_t prim_bas
   j.pano = cam.height < 0 ? 1 : 0;
   // trace_runner.cpp:131-140: shift = int(right_dir.x), times supersample_x.
   j.vr_x_shift = (int)cam.right_dir[0] * p.supersample_x;
-  j.vr_sample_x = p.sample_x * p.supersample_y;
-  j.vr_sample_y = p.sample_y * p.supersample_y;
   j.spp = p.sample;
   j.depth = p.depth;
   j.disable_diffuse = p.disable_diffuse;
@@ -588,40 +881,34 @@ DevJob Engine::make_job(const JobSpec& js, const JobBuffers& b, int64_t prim_bas
   j.flags = b.flags;
   j.prim = b.prim;
   j.prim_count = b.prim_count;
-  j.prim_base = prim_base;
-  j.counters = b.counters;
   return j;
 }
 
-hpt_status Engine::upload_jobs(const std::vector<DevJob>& jobs) {
-  if ((int)jobs.size() > jobs_cap_) {
-    cudaStreamSynchronize(stream);
-    cudaFree(jobs_);
-    jobs_ = nullptr;
-    jobs_cap_ = 0;
-    HPT_CUDA(cudaMalloc(&jobs_, jobs.size() * sizeof(DevJob)));
-    jobs_cap_ = (int)jobs.size();
-  }
-  HPT_CUDA(cudaMemcpyAsync(jobs_, jobs.data(), jobs.size() * sizeof(DevJob), cudaMemcpyHostToDevice,
-                           stream));
-  num_jobs_ = (int)jobs.size();
-  return HPT_OK;
-}
-
-static EngineParams make_params(Engine& e, DevCtrl* ctrl, DevJob* jobs, int num_jobs, int capacity,
-                                float4* const* A, int32_t* const* Atri, float4* const* R,
-                                const DevScene* shared, int64_t total_primary) {
+static EngineParams make_params(const Engine& e, DevCtrl* ctrl, DevJob* jobs, DevSlot* slots,
+                                int num_slots, const int32_t* order, int32_t* quota_slot,
+                                int32_t* quota_prefix, const int32_t* prim_slot,
+                                const int64_t* prim_prefix, int prim_n, int capacity,
+                                float4* const* A, int32_t* const* Atri, int32_t* const* Aleaf,
+                                float4* const* R, const DevScene* shared) {
   EngineParams P;
   memset(&P, 0, sizeof P);
   P.jobs = jobs;
-  P.num_jobs = num_jobs;
+  P.slots = slots;
+  P.num_slots = num_slots;
   P.ctrl = ctrl;
+  P.order = order;
+  P.quota_slot = quota_slot;
+  P.quota_prefix = quota_prefix;
+  P.prim_slot = prim_slot;
+  P.prim_prefix = prim_prefix;
+  P.prim_n = prim_n;
   for (int p = 0; p < 2; ++p) {
     P.A_o[p] = A[4 * p + 0];
     P.A_d[p] = A[4 * p + 1];
     P.A_s[p] = A[4 * p + 2];
     P.A_r[p] = A[4 * p + 3];
     P.A_tri[p] = Atri[p];
+    P.A_leaf[p] = Aleaf[p];
   }
   P.R_o = R[0];
   P.R_d = R[1];
@@ -633,72 +920,137 @@ static EngineParams make_params(Engine& e, DevCtrl* ctrl, DevJob* jobs, int num_
     P.smem_nodes = std::min(e.tuning.smem_nodes, shared->num_nodes);
     P.shared_nodes = shared->nodes;
   }
-  P.total_primary = total_primary;
   return P;
 }
 
-void Engine::launch_primary(int64_t total_primary, const DevScene* shared_scene) {
-  query_occupancy();
-  float4* A[8] = {A_o_[0], A_d_[0], A_s_[0], A_r_[0], A_o_[1], A_d_[1], A_s_[1], A_r_[1]};
-  float4* R[4] = {R_o_, R_d_, R_s_, R_r_};
-  EngineParams P = make_params(*this, ctrl_, jobs_, num_jobs_, capacity_, A, A_tri_, R,
-                               shared_scene, total_primary);
-  const size_t smem = (size_t)P.smem_nodes * sizeof(uint2);
-  k_primary<<<num_sms * occ_isect_, 256, smem, stream>>>(P);
+void Engine::reset_ctrl() {
+  HPT_SOFT(cudaMemsetAsync(ctrl_, 0, sizeof(DevCtrl), stream));
+  if (slots_ > 0) HPT_SOFT(cudaMemsetAsync(slot_state_, 0, (size_t)slots_ * sizeof(DevSlot), stream));
 }
 
-void Engine::launch_setup(int num_jobs, bool) {
-  k_setup<<<1, 1, 0, stream>>>(jobs_, num_jobs, ctrl_);
+hpt_status Engine::set_order(const std::vector<int>& order) {
+  if ((int)order.size() > slots_) return fail(HPT_ERR_INVALID_ARGUMENT, "order larger than slots");
+  // Pinned staging: [0, slots] prim_slot (admit), [slots + 1, 2 slots + 1]
+  // order, [2 slots + 2] n_order. Regions never overlap, so a copy still
+  // queued behind a kernel reads what was written for it.
+  int32_t* stage = host_i32_ + (slots_ + 1);
+  for (size_t k = 0; k < order.size(); ++k) stage[k] = order[k];
+  if (!order.empty())
+    HPT_CUDA(cudaMemcpyAsync(order_, stage, order.size() * sizeof(int32_t),
+                             cudaMemcpyHostToDevice, stream));
+  stage[slots_ + 1] = (int32_t)order.size();
+  HPT_CUDA(cudaMemcpyAsync(&ctrl_->n_order, &stage[slots_ + 1], sizeof(int32_t),
+                           cudaMemcpyHostToDevice, stream));
+  // The pinned staging is reused by the next call: wait for these copies.
+  HPT_CUDA(cudaStreamSynchronize(stream));
+  return HPT_OK;
+}
+
+hpt_status Engine::admit(const std::vector<int>& slot_ids, const std::vector<DevJob>& jobs,
+                         const std::vector<int64_t>& rays, const std::vector<int>& order,
+                         const DevScene* shared_scene) {
+  const int n = (int)slot_ids.size();
+  if (n == 0) return set_order(order);
+  {
+    hpt_status qs = query_occupancy();
+    if (qs != HPT_OK) return qs;
+  }
+  for (int k = 0; k < n; ++k) {
+    if (slot_ids[k] < 0 || slot_ids[k] >= slots_)
+      return fail(HPT_ERR_INVALID_ARGUMENT, "slot %d out of range", slot_ids[k]);
+    host_jobs_[slot_ids[k]] = jobs[k];
+    HPT_CUDA(cudaMemcpyAsync(jobs_ + slot_ids[k], host_jobs_ + slot_ids[k], sizeof(DevJob),
+                             cudaMemcpyHostToDevice, stream));
+  }
+  host_i64_[0] = 0;
+  for (int k = 0; k < n; ++k) {
+    host_i32_[k] = slot_ids[k];
+    host_i64_[k + 1] = host_i64_[k] + rays[k];
+  }
+  HPT_CUDA(cudaMemcpyAsync(prim_slot_, host_i32_, n * sizeof(int32_t), cudaMemcpyHostToDevice,
+                           stream));
+  HPT_CUDA(cudaMemcpyAsync(prim_prefix_, host_i64_, (n + 1) * sizeof(int64_t),
+                           cudaMemcpyHostToDevice, stream));
+  float4* A[8] = {A_o_[0], A_d_[0], A_s_[0], A_r_[0], A_o_[1], A_d_[1], A_s_[1], A_r_[1]};
+  float4* R[4] = {R_o_, R_d_, R_s_, R_r_};
+  EngineParams P = make_params(*this, ctrl_, jobs_, slot_state_, slots_, order_, quota_slot_,
+                               quota_prefix_, prim_slot_, prim_prefix_, n, capacity_, A, A_tri_,
+                               A_leaf_, R, shared_scene);
+  const size_t smem = (size_t)P.smem_nodes * sizeof(uint2);
+  const IsectVariant& v = kIsectVariants[isect_variant()];
+  v.primary<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
+  HPT_CUDA(cudaGetLastError());
+  hpt_status s = set_order(order);  // synchronises: the staging is free again
+  if (s != HPT_OK) return s;
+  k_admit<<<1, 1, 0, stream>>>(P);
+  HPT_CUDA(cudaGetLastError());
+  return HPT_OK;
 }
 
 void Engine::launch_iteration(const DevScene* shared_scene, cudaEvent_t* ev) {
-  query_occupancy();
   float4* A[8] = {A_o_[0], A_d_[0], A_s_[0], A_r_[0], A_o_[1], A_d_[1], A_s_[1], A_r_[1]};
   float4* R[4] = {R_o_, R_d_, R_s_, R_r_};
-  EngineParams P = make_params(*this, ctrl_, jobs_, num_jobs_, capacity_, A, A_tri_, R,
-                               shared_scene, 0);
-  if (ev) cudaEventRecord(ev[0], stream);
+  EngineParams P = make_params(*this, ctrl_, jobs_, slot_state_, slots_, order_, quota_slot_,
+                               quota_prefix_, prim_slot_, prim_prefix_, 0, capacity_, A, A_tri_,
+                               A_leaf_, R, shared_scene);
+  if (ev) HPT_SOFT(cudaEventRecord(ev[0], stream));
   k_shade<256><<<num_sms * occ_shade_, 256, 0, stream>>>(P);
-  if (ev) cudaEventRecord(ev[1], stream);
+  if (ev) HPT_SOFT(cudaEventRecord(ev[1], stream));
   const size_t smem = (size_t)P.smem_nodes * sizeof(uint2);
-  k_isect<<<num_sms * occ_isect_, 256, smem, stream>>>(P);
-  if (ev) cudaEventRecord(ev[2], stream);
-  k_ctrl<<<1, 1, 0, stream>>>(ctrl_);
+  const IsectVariant& v = kIsectVariants[isect_variant()];
+  v.isect<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
+  if (ev) HPT_SOFT(cudaEventRecord(ev[2], stream));
+  k_ctrl<<<1, 1, 0, stream>>>(P);
+}
+
+void Engine::launch_resolve(int slot, const JobSpec& js, const JobBuffers& b) {
+  const hpt_render_params& p = js.params;
+  dim3 blk(16, 16), grd((p.sample_x + 15) / 16, (p.sample_y + 15) / 16);
+  k_resolve<<<grd, blk, 0, stream>>>(jobs_ + slot, p.sample_x, p.sample_y, p.supersample_x,
+                                      p.supersample_y, p.sample, p.brightness, b.rgba, b.accum_f);
 }
 
 hpt_status Engine::run(const std::vector<JobSpec>& jobs, hpt_render_stats* stats) {
+  if (init_status_ != HPT_OK) return fail(init_status_, "engine set-up failed");
   HPT_CUDA(cudaSetDevice(device));
   if (jobs.empty()) return HPT_OK;
   hpt_status s = ensure_capacity(std::max(1024, tuning.capacity));
   if (s != HPT_OK) return s;
-  {  // smem staging must fit in the opt-in shared memory limit
-    const size_t smem = (size_t)std::max(0, tuning.smem_nodes) * sizeof(uint2);
-    cudaFuncSetAttribute(k_primary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_isect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  }
-  std::vector<JobBuffers> bufs(jobs.size());
+  s = ensure_slots((int)jobs.size());
+  if (s != HPT_OK) return s;
+  const int n = (int)jobs.size();
+  std::vector<JobBuffers> bufs(n);
   std::vector<DevJob> djobs;
-  int64_t prim_base = 0;
+  std::vector<int> slot_ids(n);
+  std::vector<int64_t> rays(n);
   const SceneDev* shared = jobs[0].scene;
-  for (size_t j = 0; j < jobs.size(); ++j) {
+  for (int j = 0; j < n; ++j) {
     s = alloc_job(jobs[j], jobs[j].accum_out != nullptr, bufs[j]);
     if (s != HPT_OK) {
-      for (size_t k = 0; k <= j; ++k) free_job(bufs[k]);
+      for (int k = 0; k <= j; ++k) free_job(bufs[k]);
       return s;
     }
-    djobs.push_back(make_job(jobs[j], bufs[j], prim_base));
-    prim_base += bufs[j].rays;
+    djobs.push_back(make_job(jobs[j], bufs[j]));
+    slot_ids[j] = j;
+    rays[j] = bufs[j].rays;
     if (jobs[j].scene != shared) shared = nullptr;
   }
-  s = upload_jobs(djobs);
-  if (s != HPT_OK) return s;
-  HPT_CUDA(cudaMemsetAsync(ctrl_, 0, sizeof(DevCtrl), stream));
+  // Smallest jobs first.
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return rays[a] * jobs[a].params.sample < rays[b] * jobs[b].params.sample;
+  });
   const DevScene* shared_dev = shared ? &shared->dev : nullptr;
-
-  cudaEventRecord(ev_[0], stream);
-  launch_primary(prim_base, shared_dev);
-  cudaEventRecord(ev_[1], stream);
-  launch_setup((int)jobs.size(), true);
+  reset_ctrl();
+  HPT_SOFT(cudaEventRecord(ev_[0], stream));
+  s = admit(slot_ids, djobs, rays, order, shared_dev);
+  if (s != HPT_OK) {
+    for (auto& b : bufs) free_job(b);
+    HPT_SOFT(cudaStreamSynchronize(stream));
+    return s;
+  }
+  HPT_SOFT(cudaEventRecord(ev_[1], stream));
   // Iterate until the device says the wavefront is drained. Batches of
   // iterations are queued ahead; the done flag of batch k is checked while
   // batch k+1 runs (extra iterations after completion are empty launches).
@@ -708,21 +1060,20 @@ hpt_status Engine::run(const std::vector<JobSpec>& jobs, hpt_render_stats* stats
   HPT_CUDA(cudaMallocHost(&done_host, 2 * sizeof(int32_t)));
   done_host[0] = done_host[1] = 0;
   cudaEvent_t ev_done[2];
-  cudaEventCreateWithFlags(&ev_done[0], cudaEventDisableTiming);
-  cudaEventCreateWithFlags(&ev_done[1], cudaEventDisableTiming);
-  // Profile mode: three events per iteration, two batches in flight.
+  HPT_SOFT(cudaEventCreateWithFlags(&ev_done[0], cudaEventDisableTiming));
+  HPT_SOFT(cudaEventCreateWithFlags(&ev_done[1], cudaEventDisableTiming));
   std::vector<cudaEvent_t> pev;
   if (prof) {
     pev.resize(2 * kBatch * 3);
-    for (auto& e : pev) cudaEventCreate(&e);
+    for (auto& e : pev) HPT_SOFT(cudaEventCreate(&e));
   }
   float ms_shade = 0.f, ms_isect = 0.f;
   auto harvest = [&](int sl) {
     for (int k = 0; k < kBatch; ++k) {
       cudaEvent_t* e = &pev[(sl * kBatch + k) * 3];
       float a = 0.f, b = 0.f;
-      cudaEventElapsedTime(&a, e[0], e[1]);
-      cudaEventElapsedTime(&b, e[1], e[2]);
+      HPT_SOFT(cudaEventElapsedTime(&a, e[0], e[1]));
+      HPT_SOFT(cudaEventElapsedTime(&b, e[1], e[2]));
       ms_shade += a;
       ms_isect += b;
     }
@@ -746,10 +1097,10 @@ hpt_status Engine::run(const std::vector<JobSpec>& jobs, hpt_render_stats* stats
   while (true) {
     for (int k = 0; k < kBatch; ++k)
       launch_iteration(shared_dev, prof ? &pev[(slot * kBatch + k) * 3] : nullptr);
-    cudaMemcpyAsync(&done_host[slot], &ctrl_->done, sizeof(int32_t), cudaMemcpyDeviceToHost, stream);
-    cudaEventRecord(ev_done[slot], stream);
+    HPT_SOFT(cudaMemcpyAsync(&done_host[slot], &ctrl_->done, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+    HPT_SOFT(cudaEventRecord(ev_done[slot], stream));
     if (pending) {
-      cudaEventSynchronize(ev_done[slot ^ 1]);
+      HPT_SOFT(cudaEventSynchronize(ev_done[slot ^ 1]));
       if (prof) harvest(slot ^ 1);
       if (done_host[slot ^ 1]) {
         drained = true;
@@ -760,61 +1111,65 @@ hpt_status Engine::run(const std::vector<JobSpec>& jobs, hpt_render_stats* stats
     slot ^= 1;
     if (++guard > max_batches) break;
   }
-  cudaEventRecord(ev_[2], stream);
-  for (size_t j = 0; j < jobs.size(); ++j) {
-    const hpt_render_params& p = jobs[j].params;
-    dim3 blk(16, 16), grd((p.sample_x + 15) / 16, (p.sample_y + 15) / 16);
-    k_resolve<<<grd, blk, 0, stream>>>(jobs_ + j, p.sample_x, p.sample_y, p.supersample_x,
-                                        p.supersample_y, p.brightness, bufs[j].rgba,
-                                        bufs[j].accum_f);
-  }
-  cudaEventRecord(ev_[3], stream);
-  for (size_t j = 0; j < jobs.size(); ++j) {
+  HPT_SOFT(cudaEventRecord(ev_[2], stream));
+  for (int j = 0; j < n; ++j) launch_resolve(j, jobs[j], bufs[j]);
+  HPT_SOFT(cudaEventRecord(ev_[3], stream));
+  for (int j = 0; j < n; ++j) {
     const hpt_render_params& p = jobs[j].params;
     if (jobs[j].rgba_out)
-      cudaMemcpyAsync(jobs[j].rgba_out, bufs[j].rgba, (size_t)p.sample_x * p.sample_y * 4,
-                      cudaMemcpyDeviceToHost, stream);
+      HPT_SOFT(cudaMemcpyAsync(jobs[j].rgba_out, bufs[j].rgba, (size_t)p.sample_x * p.sample_y * 4, cudaMemcpyDeviceToHost, stream));
     if (jobs[j].accum_out)
-      cudaMemcpyAsync(jobs[j].accum_out, bufs[j].accum_f, (size_t)bufs[j].rays * 3 * sizeof(float),
-                      cudaMemcpyDeviceToHost, stream);
+      HPT_SOFT(cudaMemcpyAsync(jobs[j].accum_out, bufs[j].accum_f, (size_t)bufs[j].rays * 3 * sizeof(float), cudaMemcpyDeviceToHost, stream));
   }
-  cudaMemcpyAsync(ctrl_host_, ctrl_, sizeof(DevCtrl), cudaMemcpyDeviceToHost, stream);
+  HPT_SOFT(cudaMemcpyAsync(ctrl_host_, ctrl_, sizeof(DevCtrl), cudaMemcpyDeviceToHost, stream));
   for (auto& b : bufs) free_job(b);
   cudaError_t e = cudaStreamSynchronize(stream);
   if (prof) harvest(slot);
-  for (auto& ev : pev) cudaEventDestroy(ev);
-  cudaEventDestroy(ev_done[0]);
-  cudaEventDestroy(ev_done[1]);
-  cudaFreeHost(done_host);
+  for (auto& ev : pev) HPT_SOFT(cudaEventDestroy(ev));
+  HPT_SOFT(cudaEventDestroy(ev_done[0]));
+  HPT_SOFT(cudaEventDestroy(ev_done[1]));
+  HPT_SOFT(cudaFreeHost(done_host));
   if (e != cudaSuccess) return cuda_fail(e, "render");
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "render launch");
+  int64_t prim = 0;
+  for (int64_t r : rays) prim += r;
   if (stats) {
     memset(stats, 0, sizeof *stats);
-    stats->primary_rays = prim_base;
+    stats->primary_rays = prim;
     stats->intersect_queries = (int64_t)ctrl_host_->isect_queries;
     stats->shade_calls = (int64_t)ctrl_host_->shades;
-    stats->paths = ctrl_host_->total_paths;
     stats->iterations = (int32_t)ctrl_host_->iterations;
-    stats->error_flags = (int32_t)ctrl_host_->error;
-    cudaEventElapsedTime(&stats->ms_total, ev_[0], ev_[3]);
-    cudaEventElapsedTime(&stats->ms_primary, ev_[0], ev_[1]);
-    cudaEventElapsedTime(&stats->ms_loop, ev_[1], ev_[2]);
+    stats->error_flags = (int32_t)ctrl_host_->err.flags;
+    HPT_SOFT(cudaEventElapsedTime(&stats->ms_total, ev_[0], ev_[3]));
+    HPT_SOFT(cudaEventElapsedTime(&stats->ms_primary, ev_[0], ev_[1]));
+    HPT_SOFT(cudaEventElapsedTime(&stats->ms_loop, ev_[1], ev_[2]));
     stats->ms_shade = prof ? ms_shade : -1.f;
     stats->ms_intersect = prof ? ms_isect : -1.f;
-    cudaEventElapsedTime(&stats->ms_resolve, ev_[2], ev_[3]);
+    HPT_SOFT(cudaEventElapsedTime(&stats->ms_resolve, ev_[2], ev_[3]));
     stats->nodes_visited = (int64_t)ctrl_host_->nodes_visited;
     stats->leaves_visited = (int64_t)ctrl_host_->leaves_visited;
     stats->triangle_tests = (int64_t)ctrl_host_->tri_tests;
+    stats->triangle_repeats = (int64_t)ctrl_host_->tri_repeats;
+    std::vector<DevSlot> st(n);
+    const cudaError_t ce =
+        cudaMemcpy(st.data(), slot_state_, n * sizeof(DevSlot), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) cuda_soft_fail(ce, "slot state read-back");
+    if (ce == cudaSuccess) {
+      int64_t paths = 0;
+      for (const DevSlot& x : st) paths += x.num_paths;
+      stats->paths = paths;
+    }
   }
-  if (ctrl_host_->error) return fail(HPT_ERR_TRAVERSAL_LIMIT, "a traversal hit its step cap");
+  if (ctrl_host_->err.flags & 2u)
+    return fail(HPT_ERR_INVALID_SCENE, "device self-check %d failed (value %lld)",
+                ctrl_host_->err.site, (long long)ctrl_host_->err.value);
+  if (ctrl_host_->err.flags & 1u)
+    return fail(HPT_ERR_TRAVERSAL_LIMIT, "a traversal hit its step cap");
   if (!drained && !ctrl_host_->done)
     return fail(HPT_ERR_TRAVERSAL_LIMIT, "the wavefront did not drain within %lld iterations",
                 (long long)(max_batches * kBatch));
   return HPT_OK;
 }
 
-// ---------------------------------------------------------------------------
-// Scene upload
-// ---------------------------------------------------------------------------
 }  // namespace hpt

@@ -13,6 +13,9 @@
 
 namespace hpt {
 
+// Largest shared-memory node prefix a tuning may ask for (64 KB).
+constexpr int kMaxSmemNodes = 8192;
+
 struct SceneDev {
   int device = 0;
   DevScene dev;              // device pointers (host copy)
@@ -22,7 +25,7 @@ struct SceneDev {
   int64_t bytes = 0;
 };
 
-// One render request inside a wavefront run.
+// One render request.
 struct JobSpec {
   const SceneDev* scene = nullptr;
   hpt_camera camera{};
@@ -31,27 +34,28 @@ struct JobSpec {
   float* accum_out = nullptr;    // host, may be null
 };
 
-// Per-job device buffers, owned by the engine for the duration of a run
-// (or of a request in the server).
+// Per-job device buffers (owned by the engine while the job runs).
 struct JobBuffers {
   unsigned long long* accum = nullptr;  // 3 per ray, fixed point
   uint32_t* flags = nullptr;            // non-finite markers per ray
   float* prim = nullptr;                // primary hit cache
   int32_t* prim_count = nullptr;
-  unsigned long long* counters = nullptr;
   uint8_t* rgba = nullptr;
   float* accum_f = nullptr;
   int64_t rays = 0;
   int64_t bytes = 0;
 };
 
+// Device bytes a job needs besides the shared wavefront (admission control).
+int64_t job_footprint(const hpt_render_params& p, bool want_accum);
+
 class Engine {
  public:
   explicit Engine(int device);
   ~Engine();
 
-  // Renders all jobs in one wavefront (primary pass for all jobs, then
-  // paths of every job interleaved in the same queues).
+  // Renders all jobs in one wavefront: primary pass for every job, then the
+  // paths of all jobs share the queues (smallest job first).
   hpt_status run(const std::vector<JobSpec>& jobs, hpt_render_stats* stats);
 
   hpt_tuning tuning;
@@ -59,41 +63,59 @@ class Engine {
   cudaStream_t stream = nullptr;
   int num_sms = 0;
 
-  // --- pieces shared with the server ------------------------------------
+  // --- building blocks (also used by the server) --------------------------
   hpt_status ensure_capacity(int capacity);
+  hpt_status ensure_slots(int slots);
+  int slots() const { return slots_; }
   hpt_status alloc_job(const JobSpec& js, bool want_accum, JobBuffers& b);
   void free_job(JobBuffers& b);
-  DevJob make_job(const JobSpec& js, const JobBuffers& b, int64_t prim_base) const;
-  // Enqueue helpers (stream-ordered, no sync).
-  hpt_status upload_jobs(const std::vector<DevJob>& jobs);
-  void launch_primary(int64_t total_primary, const DevScene* shared_scene);
-  void launch_setup(int num_jobs, bool reset_cursor);
+  DevJob make_job(const JobSpec& js, const JobBuffers& b) const;
+  // Stream-ordered: writes the jobs into their slots, runs their primary
+  // pass and grants them paths. `order` lists every active slot, highest
+  // priority first.
+  hpt_status admit(const std::vector<int>& slot_ids, const std::vector<DevJob>& jobs,
+                   const std::vector<int64_t>& rays, const std::vector<int>& order,
+                   const DevScene* shared_scene);
+  hpt_status set_order(const std::vector<int>& order);
   void launch_iteration(const DevScene* shared_scene, cudaEvent_t* ev3 = nullptr);
+  void launch_resolve(int slot, const JobSpec& js, const JobBuffers& b);
+  void reset_ctrl();
   DevCtrl* ctrl_dev() const { return ctrl_; }
-  DevJob* jobs_dev() const { return jobs_; }
-  int num_jobs_dev() const { return num_jobs_; }
+  DevSlot* slots_dev() const { return slot_state_; }
+  int isect_variant() const;  // index into the traversal kernel variants
 
  private:
   int capacity_ = 0;
+  int slots_ = 0;
   DevCtrl* ctrl_ = nullptr;
   DevCtrl* ctrl_host_ = nullptr;  // pinned
   DevJob* jobs_ = nullptr;
-  int jobs_cap_ = 0;
-  int num_jobs_ = 0;
+  DevSlot* slot_state_ = nullptr;
+  int32_t* order_ = nullptr;
+  int32_t* quota_slot_ = nullptr;
+  int32_t* quota_prefix_ = nullptr;
+  int32_t* prim_slot_ = nullptr;
+  int64_t* prim_prefix_ = nullptr;
+  int32_t* host_i32_ = nullptr;   // pinned staging for small uploads
+  int64_t* host_i64_ = nullptr;
+  DevJob* host_jobs_ = nullptr;
   // Shade queues (double-buffered) and the intersect queue.
   float4* A_o_[2] = {nullptr, nullptr};
   float4* A_d_[2] = {nullptr, nullptr};
   float4* A_s_[2] = {nullptr, nullptr};
   float4* A_r_[2] = {nullptr, nullptr};
   int32_t* A_tri_[2] = {nullptr, nullptr};
+  int32_t* A_leaf_[2] = {nullptr, nullptr};
   float4* R_o_ = nullptr;
   float4* R_d_ = nullptr;
   float4* R_s_ = nullptr;
   float4* R_r_ = nullptr;
   cudaEvent_t ev_[6];
+  hpt_status init_status_ = HPT_OK;
+  hpt_status init();
   int occ_isect_ = 1, occ_shade_ = 1;
   bool occ_done_ = false;
-  void query_occupancy();
+  hpt_status query_occupancy();
 };
 
 struct SceneHandle {
@@ -102,12 +124,12 @@ struct SceneHandle {
   std::unique_ptr<Engine> engine;
   hpt_render_stats last_stats{};
   hpt_tuning tuning{};
-  bool tuning_set = false;
 };
 
 hpt_status upload_scene(const hpt_scene_desc& desc, SceneDev& out);
 void release_scene(SceneDev& s);
 hpt_tuning default_tuning();
+hpt_status check_render_params(const hpt_camera* cam, const hpt_render_params* p);
 
 // CUDA error -> hpt_status with message.
 hpt_status cuda_fail(cudaError_t e, const char* what);
@@ -115,6 +137,17 @@ hpt_status cuda_fail(cudaError_t e, const char* what);
   do {                                                      \
     cudaError_t e_ = (call);                                \
     if (e_ != cudaSuccess) return ::hpt::cuda_fail(e_, #call); \
+  } while (0)
+
+// Best-effort call (teardown, timing, stream-ordered frees): its error is
+// not returned, but it is cleared from the runtime's per-thread error state
+// so that a later launch check does not report it as its own. Self-check
+// builds print it.
+void cuda_soft_fail(cudaError_t e, const char* what);
+#define HPT_SOFT(call)                                   \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) ::hpt::cuda_soft_fail(e_, #call); \
   } while (0)
 
 }  // namespace hpt

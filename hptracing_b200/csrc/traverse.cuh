@@ -18,6 +18,7 @@
 // lose its true closest hit in the reference, never here.
 #pragma once
 
+#include "checks.cuh"
 #include "device_types.h"
 #include "dmath.cuh"
 
@@ -29,33 +30,23 @@ struct Hit {
   float t, u, v;
 };
 
-// _box_intersect (kernel.cl:56-83) with the slab distances kept for the
-// exit computation: returns the reference's verdict; t_exit is the
-// smallest far-slab distance over axes with a non-zero direction and
-// exit_face its face (2*axis + 1 if leaving through the high side).
-__device__ __forceinline__ bool leaf_slabs(const Ray& r, const float lo[3], const float hi[3],
-                                           float& t_exit, int& exit_face) {
+// _box_intersect (kernel.cl:56-83), exactly: origin-inside shortcut, then
+// slabs (s - p0) / p with IEEE division, fmin/fmax, min_of_maxs <= 0 -> miss.
+HPT_HD bool ref_box_test(const Ray& r, const float4 lo, const float4 hi) {
   const float o[3] = {r.o.x, r.o.y, r.o.z};
   const float d[3] = {r.d.x, r.d.y, r.d.z};
+  const float l[3] = {lo.x, lo.y, lo.z};
+  const float h[3] = {hi.x, hi.y, hi.z};
   bool inside = true;
   float max_of_mins = 0.f, min_of_maxs = 0.f;
-  t_exit = __int_as_float(0x7f800000);  // +inf
-  exit_face = -1;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    inside = inside && o[a] >= lo[a] && o[a] <= hi[a];
-    float t0 = __fdiv_rn(__fsub_rn(lo[a], o[a]), d[a]);
-    float t1 = __fdiv_rn(__fsub_rn(hi[a], o[a]), d[a]);
-    float mn = fminf(t0, t1), mx = fmaxf(t0, t1);
+    inside = inside && o[a] >= l[a] && o[a] <= h[a];
+    const float t0 = rn_div(rn_sub(l[a], o[a]), d[a]);
+    const float t1 = rn_div(rn_sub(h[a], o[a]), d[a]);
+    const float mn = fminf(t0, t1), mx = fmaxf(t0, t1);
     max_of_mins = a == 0 ? mn : fmaxf(max_of_mins, mn);
     min_of_maxs = a == 0 ? mx : fminf(min_of_maxs, mx);
-    if (d[a] != 0.f) {
-      float tf = d[a] > 0.f ? t1 : t0;
-      if (tf < t_exit) {
-        t_exit = tf;
-        exit_face = 2 * a + (d[a] > 0.f ? 1 : 0);
-      }
-    }
   }
   if (inside) return true;
   if (min_of_maxs <= 0.f) return false;
@@ -64,19 +55,19 @@ __device__ __forceinline__ bool leaf_slabs(const Ray& r, const float lo[3], cons
 
 // _single_intersect (kernel.cl:85-109) on a pre-subtracted record. The
 // epsilon test at kernel.cl:93 can never be true and is omitted.
-__device__ __forceinline__ bool mt_test(const Ray& r, const float4 A, const float4 E1,
+HPT_HD bool mt_test(const Ray& r, const float4 A, const float4 E1,
                                         const float4 E2, float& t, float& u, float& v) {
   f3 a = mk(A.x, A.y, A.z), e1 = mk(E1.x, E1.y, E1.z), e2 = mk(E2.x, E2.y, E2.z);
   f3 P = cross(r.d, e2);
   float det = dot(e1, P);
-  float inv_det = __fdiv_rn(1.f, det);
+  float inv_det = rn_div(1.f, det);
   f3 T = sub(r.o, a);
-  u = __fmul_rn(dot(T, P), inv_det);
+  u = rn_mul(dot(T, P), inv_det);
   if (u < 0.f || u > 1.f) return false;
   f3 Q = cross(T, e1);
-  v = __fmul_rn(dot(r.d, Q), inv_det);
-  if (v < 0.f || __fadd_rn(u, v) > 1.f) return false;
-  t = __fmul_rn(dot(e2, Q), inv_det);
+  v = rn_mul(dot(r.d, Q), inv_det);
+  if (v < 0.f || rn_add(u, v) > 1.f) return false;
+  t = rn_mul(dot(e2, Q), inv_det);
   return t > 0.f;
 }
 
@@ -84,37 +75,53 @@ __device__ __forceinline__ bool mt_test(const Ray& r, const float4 A, const floa
 // refilled with a new ray between leaves.
 struct TravState {
   Ray ray;
+  f3 inv_d;              // 1 / d (exit distances only; the filter divides)
   float t_entry, t_end;  // current entry distance, scene exit distance
   float slack;           // world-space rounding slack in t units
   int32_t node;          // node to descend from, -1 = finished
   int32_t steps;
+  int32_t best_node;     // leaf node where the best hit was found
   Hit best;
+  // The last four triangles tested and their Moller-Trumbore t (-1 = miss):
+  // the reference tree repeats a triangle in every leaf it straddles.
+  int32_t mb_id[4];
+  float mb_t[4];
 };
 
 // Work counters of one lane (summed over the rays it traced).
 struct TravCount {
-  unsigned long long nodes = 0, leaves = 0, tris = 0;
+  unsigned long long nodes = 0, leaves = 0, tris = 0, repeats = 0;
 };
 
-__device__ __forceinline__ void trav_init(const DevScene& s, const Ray& r, TravState& st) {
+// Starts a query. start_node (>= 0) names a leaf node the origin is
+// expected to lie in (the leaf of the previous hit): if its box contains the
+// origin the walk starts there instead of descending from the root.
+HPT_HD void trav_init(const DevScene& s, const Ray& r, TravState& st,
+                                          int start_node = -1) {
   st.ray = r;
   st.best.rec = -1;
   st.best.tri = -1;
   st.best.t = 0.f;
   st.best.u = st.best.v = 0.f;
+  st.best_node = -1;
   st.steps = 0;
   st.node = -1;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    st.mb_id[k] = -1;
+    st.mb_t[k] = -1.f;
+  }
   if (!finite3(r.o) || !finite3(r.d)) return;
   const float o[3] = {r.o.x, r.o.y, r.o.z};
   const float d[3] = {r.d.x, r.d.y, r.d.z};
-  float t0 = 0.f, t1 = __int_as_float(0x7f800000);
+  float t0 = 0.f, t1 = as_float(0x7f800000);
   float dmax = 0.f;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     dmax = fmaxf(dmax, fabsf(d[a]));
     if (d[a] != 0.f) {
-      float ta = __fdiv_rn(__fsub_rn(s.root_lo[a], o[a]), d[a]);
-      float tb = __fdiv_rn(__fsub_rn(s.root_hi[a], o[a]), d[a]);
+      float ta = rn_div(rn_sub(s.root_lo[a], o[a]), d[a]);
+      float tb = rn_div(rn_sub(s.root_hi[a], o[a]), d[a]);
       t0 = fmaxf(t0, fminf(ta, tb));
       t1 = fminf(t1, fmaxf(ta, tb));
     } else if (o[a] < s.root_lo[a] || o[a] > s.root_hi[a]) {
@@ -122,73 +129,147 @@ __device__ __forceinline__ void trav_init(const DevScene& s, const Ray& r, TravS
     }
   }
   if (!(dmax > 0.f) || !(t0 <= t1)) return;
+  st.inv_d = mk(rn_rcp(r.d.x), rn_rcp(r.d.y), rn_rcp(r.d.z));
   st.t_entry = t0;
   st.t_end = t1;
-  st.slack = __fdiv_rn(s.scene_eps, dmax);
+  st.slack = rn_div(s.scene_eps, dmax);
   st.node = 0;
+  if (start_node > 0 && start_node < s.num_nodes) {
+    const uint2 nd = ldg(reinterpret_cast<const uint2*>(s.nodes) + start_node);
+    if ((nd.x >> 30) == kLeafKind) {
+      const float4* L = reinterpret_cast<const float4*>(s.leaves + (nd.x & kIndexMask));
+      const float4 lo = ldg(L), hi = ldg(L + 1);
+      if (o[0] >= lo.x && o[0] <= hi.x && o[1] >= lo.y && o[1] <= hi.y && o[2] >= lo.z &&
+          o[2] <= hi.z) {
+        st.node = start_node;
+        st.t_entry = 0.f;
+      }
+    }
+  }
 }
 
 // Node fetch with an optional shared-memory copy of the first n_smem nodes.
-__device__ __forceinline__ uint2 fetch_node(const DevScene& s, const uint2* smem, int n_smem,
+HPT_HD uint2 fetch_node(const DevScene& s, const uint2* smem, int n_smem,
                                             int i) {
   if (i < n_smem) return smem[i];
-  return __ldg(reinterpret_cast<const uint2*>(s.nodes) + i);
+  return ldg(reinterpret_cast<const uint2*>(s.nodes) + i);
 }
+
+// A node that ends the walk (used when a self-check rejects an index).
+constexpr uint32_t kDeadLeafMeta = 0xFFFFFFFFu;
 
 // Processes one leaf: descends from st.node to the leaf containing the
 // entry point, tests its triangles, then follows the exit rope.
 // Returns true when the ray is finished.
-__device__ __forceinline__ bool trav_leaf(const DevScene& s, TravState& st, const uint2* smem,
-                                          int n_smem, uint32_t* err, TravCount& cnt) {
+// kUV: also report the winning test's Moller-Trumbore u, v (stage entry).
+template <bool kUV = false>
+HPT_HD bool trav_leaf(const DevScene& s, TravState& st, const uint2* smem,
+                                          int n_smem, DevErr* err, TravCount& cnt) {
   if (st.node < 0) return true;
+  HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
   const Ray& r = st.ray;
   // Entry point p = o + t_entry * d (kernel.cl:291 style, no FMA).
-  const float px = __fadd_rn(r.o.x, __fmul_rn(st.t_entry, r.d.x));
-  const float py = __fadd_rn(r.o.y, __fmul_rn(st.t_entry, r.d.y));
-  const float pz = __fadd_rn(r.o.z, __fmul_rn(st.t_entry, r.d.z));
+  const float px = rn_add(r.o.x, rn_mul(st.t_entry, r.d.x));
+  const float py = rn_add(r.o.y, rn_mul(st.t_entry, r.d.y));
+  const float pz = rn_add(r.o.z, rn_mul(st.t_entry, r.d.z));
   int node = st.node;
   uint2 nd = fetch_node(s, smem, n_smem, node);
   while ((nd.x >> 30) != kLeafKind) {
     const uint32_t axis = nd.x >> 30;
-    const float split = __uint_as_float(nd.y);
+    const float split = as_float_u(nd.y);
     const float p = axis == 0 ? px : (axis == 1 ? py : pz);
     const float dd = axis == 0 ? r.d.x : (axis == 1 ? r.d.y : r.d.z);
     const bool right = p > split || (p == split && dd > 0.f);
+    HPT_DCHECK(err, (int)(nd.x & kIndexMask) + 1 < s.num_nodes, 106, nd.x & kIndexMask,
+               { st.node = -1; return true; });
     node = (int)(nd.x & kIndexMask) + (right ? 1 : 0);
     nd = fetch_node(s, smem, n_smem, node);
     ++cnt.nodes;
     if (++st.steps > s.max_steps) {
-      atomicOr(err, 1u);
+      hpt_atomic_or(&err->flags, 1u);
       st.node = -1;
       return true;
     }
   }
+  HPT_DCHECK(err, (int)(nd.x & kIndexMask) < s.num_leaves, 102, nd.x & kIndexMask,
+             { st.node = -1; return true; });
   const DevLeaf* L = s.leaves + (nd.x & kIndexMask);
-  const float4 L0 = __ldg(reinterpret_cast<const float4*>(L));
-  const float4 L1 = __ldg(reinterpret_cast<const float4*>(L) + 1);
-  const float lo[3] = {L0.x, L0.y, L0.z};
-  const float hi[3] = {L1.x, L1.y, L1.z};
-  float t_exit;
-  int face;
-  const bool pierced = leaf_slabs(r, lo, hi, t_exit, face);
-  const int begin = __float_as_int(L0.w), count = __float_as_int(L1.w);
+  const float4 L0 = ldg(reinterpret_cast<const float4*>(L));
+  const float4 L1 = ldg(reinterpret_cast<const float4*>(L) + 1);
+  // Exit distance and face (reciprocal multiplies; only the reference's box
+  // filter below needs the division form).
+  float t_exit = as_float(0x7f800000);
+  int face = -1;
+  {
+    const float d[3] = {r.d.x, r.d.y, r.d.z};
+    const float o[3] = {r.o.x, r.o.y, r.o.z};
+    const float iv[3] = {st.inv_d.x, st.inv_d.y, st.inv_d.z};
+    const float lo[3] = {L0.x, L0.y, L0.z};
+    const float hi[3] = {L1.x, L1.y, L1.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (d[a] != 0.f) {
+        const float tf = rn_mul(rn_sub(d[a] > 0.f ? hi[a] : lo[a], o[a]), iv[a]);
+        if (tf < t_exit) {
+          t_exit = tf;
+          face = 2 * a + (d[a] > 0.f ? 1 : 0);
+        }
+      }
+    }
+  }
+  const int begin = as_int(L0.w), count = as_int(L1.w);
   ++cnt.leaves;
-  if (pierced && count > 0) {
-    cnt.tris += (unsigned)count;
+  HPT_DCHECK(err, begin >= 0 && count >= 0 && (long long)begin + count <= s.num_leaf_tris, 103,
+             begin, { st.node = -1; return true; });
+  if (count > 0) {
+    // The reference only considers triangles of leaves whose box passes
+    // _box_intersect; evaluated once, when a candidate would win.
+    int pierced = -1;
     const int32_t* ids = s.leaf_refs + begin;
     const float4* recs = reinterpret_cast<const float4*>(s.tris);
     for (int k = 0; k < count; ++k) {
-      const float4* rec = recs + 3 * (size_t)__ldg(ids + k);
-      const float4 A = __ldg(rec), E1 = __ldg(rec + 1), E2 = __ldg(rec + 2);
-      float t, u, v;
-      if (mt_test(r, A, E1, E2, t, u, v)) {
-        const int j = begin + k;
-        if (st.best.rec < 0 || t < st.best.t || (t == st.best.t && j < st.best.rec)) {
+      const int id = ldg(ids + k);
+      const int j = begin + k;
+      HPT_DCHECK(err, id >= 0 && id < s.num_triangles, 104, id, continue);
+      float t = -1.f, u = 0.f, v = 0.f;
+      bool tested = false;
+      int slot = -1;
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+        if (st.mb_id[m] == id) slot = m;
+      if (slot >= 0) {
+        ++cnt.repeats;
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+          if (m == slot) t = st.mb_t[m];
+      } else {
+        ++cnt.tris;
+        const float4* rec = recs + 3 * (size_t)id;
+        const float4 A = ldg(rec), E1 = ldg(rec + 1), E2 = ldg(rec + 2);
+        if (!mt_test(r, A, E1, E2, t, u, v)) t = -1.f;
+        tested = true;
+        st.mb_id[3] = st.mb_id[2]; st.mb_t[3] = st.mb_t[2];
+        st.mb_id[2] = st.mb_id[1]; st.mb_t[2] = st.mb_t[1];
+        st.mb_id[1] = st.mb_id[0]; st.mb_t[1] = st.mb_t[0];
+        st.mb_id[0] = id; st.mb_t[0] = t;
+      }
+      if (t > 0.f &&
+          (st.best.rec < 0 || t < st.best.t || (t == st.best.t && j < st.best.rec))) {
+        if (pierced < 0) pierced = ref_box_test(r, L0, L1) ? 1 : 0;
+        if (pierced) {
+          if (kUV && !tested) {  // a repeat that now wins: recover its u, v
+            const float4* rec = recs + 3 * (size_t)id;
+            float t2;
+            mt_test(r, ldg(rec), ldg(rec + 1), ldg(rec + 2), t2, u, v);
+          }
           st.best.rec = j;
-          st.best.tri = __float_as_int(A.w);
+          st.best.tri = id;
           st.best.t = t;
-          st.best.u = u;
-          st.best.v = v;
+          if (kUV) {
+            st.best.u = u;
+            st.best.v = v;
+          }
+          st.best_node = node;
         }
       }
     }
@@ -197,16 +278,17 @@ __device__ __forceinline__ bool trav_leaf(const DevScene& s, TravState& st, cons
   // Stop once the rest of the ray starts beyond the best hit (+ slack).
   if (face < 0 || !(t_exit < st.t_end)) { st.node = -1; return true; }
   if (st.best.rec >= 0 &&
-      t_exit > __fadd_rn(st.best.t, __fadd_rn(__fmul_rn(st.best.t, 1e-4f), st.slack))) {
+      t_exit > rn_add(st.best.t, rn_add(rn_mul(st.best.t, 1e-4f), st.slack))) {
     st.node = -1;
     return true;
   }
-  const int rope = __ldg(reinterpret_cast<const int*>(L) + 8 + face);
+  const int rope = ldg(reinterpret_cast<const int*>(L) + 8 + face);
   if (rope < 0 || st.steps > s.max_steps) {
-    if (rope >= 0) atomicOr(err, 1u);
+    if (rope >= 0) hpt_atomic_or(&err->flags, 1u);
     st.node = -1;
     return true;
   }
+  HPT_DCHECK(err, rope < s.num_nodes, 105, rope, { st.node = -1; return true; });
   st.node = rope;
   st.t_entry = fmaxf(st.t_entry, t_exit);
   return false;

@@ -248,7 +248,8 @@ typedef struct hpt_render_stats {
   float ms_loop;              /* all wavefront iterations                */
   int64_t nodes_visited;      /* inner nodes descended, all queries      */
   int64_t leaves_visited;
-  int64_t triangle_tests;
+  int64_t triangle_tests;     /* Moller-Trumbore tests run               */
+  int64_t triangle_repeats;   /* leaf references skipped as already tested */
 } hpt_render_stats;
 
 /* rgba_out: sample_x * sample_y * 4 bytes, layout of get_image
@@ -264,13 +265,13 @@ hpt_status hpt_render_stats_get(const hpt_scene* scene, hpt_render_stats* out);
 /* Engine tuning knobs (defaults come from the autotuner cache when set). */
 typedef struct hpt_tuning {
   int32_t capacity;          /* paths in flight (wavefront size)          */
-  int32_t isect_block;       /* threads per intersect block               */
+  int32_t isect_block;       /* threads per intersect block (128 / 256)   */
   int32_t shade_block;       /* threads per shade block                   */
   int32_t refill_chunk;      /* lanes idle before a warp refills          */
   int32_t smem_nodes;        /* top-of-tree nodes staged in shared memory */
   int32_t use_graph;         /* capture the bounce loop in a CUDA graph   */
   int32_t profile;           /* time each stage with CUDA events          */
-  int32_t reserved;
+  int32_t isect_min_blocks;  /* register budget: blocks per SM to fit     */
 } hpt_tuning;
 hpt_status hpt_tuning_get(const hpt_scene* scene, hpt_tuning* out);
 hpt_status hpt_tuning_set(hpt_scene* scene, const hpt_tuning* in);

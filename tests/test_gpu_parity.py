@@ -76,18 +76,24 @@ def test_intersect_secondary_rays(spheres):
 
 
 def test_intersect_fp32_vs_fp64(room):
-    """States the FP32 hit-distance error against an FP64 brute force."""
+    """States the FP32 hit-distance error against an FP64 brute force.
+    Different triangles are only allowed as shared-edge ties (same t)."""
     _, gpu, cpu = room
     o, d = _rays("random", 20000)
     tri, t, _, _ = gpu.intersect(o, d)
     btri, bt = cpu.brute_f64(o, d)
+    assert ((tri >= 0) == (btri >= 0)).mean() > 0.9999
     both = (tri >= 0) & (btri >= 0)
     rel = np.abs(t[both] - bt[both]) / np.maximum(bt[both], 1e-6)
-    same = (tri == btri).mean()
-    print("fp32 vs fp64: same triangle %.5f, max rel t err %.3g, p99 %.3g"
-          % (same, rel.max(), np.percentile(rel, 99)))
-    assert same > 0.999
+    other = (tri != btri)[both]
+    print("fp32 vs fp64: hit agreement %.5f, same triangle %.5f (rest are edge ties), "
+          "rel t err max %.3g p99 %.3g p99.9 %.3g"
+          % (((tri >= 0) == (btri >= 0)).mean(), 1 - other.mean(), rel.max(),
+             np.percentile(rel, 99), np.percentile(rel, 99.9)))
     assert np.percentile(rel, 99) < 1e-5
+    assert rel.max() < 1e-3
+    if other.any():
+        assert rel[other].max() < 1e-5
 
 
 def _hits(cpu, n, seed):

@@ -1,0 +1,132 @@
+"""CPU tests of the GPU per-ray code: traverse.cuh and shading.cuh are built
+for the host (tests/hostemu, with the device self-checks on) over the same
+packed tree the kernels read, and compared bit for bit with the oracle.
+
+This checks the packer (8-byte nodes, re-inserted empty slabs, ropes, leaf
+records), the stackless traversal with start-leaf hints and the shared-memory
+node prefix, the mailbox and the tie ranks, without a GPU. The GPU tests run
+the same functions compiled for sm_100a."""
+import numpy as np
+import pytest
+
+import oracle as O
+from tests import scenes as S
+
+emu = pytest.importorskip("tests.hostemu")
+
+
+@pytest.fixture(scope="module", params=[(0, {}), (1, dict(seed=1, texture_size=32))],
+                ids=["room", "spheres"])
+def pair(request):
+    cfg, kw = request.param
+    mesh, nodes, leaf = S.make_scene(cfg, **kw)
+    return O.CpuScene(mesh, nodes, leaf), emu.EmuScene(mesh, nodes, leaf)
+
+
+def _same_hits(ref, got):
+    ok = ref["overflow"] == 0
+    assert ok.mean() > 0.999
+    for k in ("tri", "t", "u", "v"):
+        a, b = ref[k][ok], got[k][ok]
+        bad = np.flatnonzero(a.view(np.int32) != b.view(np.int32))
+        assert bad.size == 0, (k, bad[:5], a[bad[:5]], b[bad[:5]])
+
+
+def _rays(kind):
+    if kind == "camera":
+        return O.raygen(S.ROOM_CAM, 96, 64, 1, 1)
+    if kind == "pano":
+        return O.raygen(S.PANO_CAM, 64, 32, 1, 1)
+    return S.random_rays(8000, seed=3)
+
+
+@pytest.mark.parametrize("kind", ["camera", "pano", "random"])
+@pytest.mark.parametrize("smem", [0, 2048])
+def test_traversal_matches_oracle(pair, kind, smem):
+    cs, em = pair
+    o, d = _rays(kind)
+    got = em.intersect(o, d, smem_nodes=smem)
+    assert got["err"][0] == 0, got["err"]
+    _same_hits(cs.intersect(o, d), got)
+
+
+def test_hinted_secondary_rays_match_oracle(pair):
+    """Secondary rays started from the leaf of the previous hit (the kernels'
+    start-leaf hint) find the same closest hit as a traversal from the root."""
+    cs, em = pair
+    o, d = S.random_rays(8000, seed=7)
+    first = em.intersect(o, d)
+    h = first["tri"] >= 0
+    p = o[h] + first["t"][h, None] * d[h]
+    rng = np.random.default_rng(5)
+    nd = rng.normal(size=p.shape).astype(np.float32)
+    nd /= np.linalg.norm(nd, axis=1, keepdims=True)
+    for eps in (0.0, 1e-5, 1e-3):
+        o2 = (p + np.float32(eps) * nd).astype(np.float32)
+        ref = cs.intersect(o2, nd)
+        hinted = em.intersect(o2, nd, hints=first["node"][h], smem_nodes=2048)
+        assert hinted["err"][0] == 0, hinted["err"]
+        _same_hits(ref, hinted)
+        plain = em.intersect(o2, nd)
+        # a hint never costs more node visits than starting at the root
+        assert hinted["counts"][0] <= plain["counts"][0]
+
+
+def test_bad_hints_fall_back_to_root(pair):
+    """A hint that is not a leaf node of this tree is ignored."""
+    cs, em = pair
+    o, d = S.random_rays(2000, seed=11)
+    n = em.counts()["nodes"]
+    hints = np.random.default_rng(2).integers(-5, n + 5, len(o)).astype(np.int32)
+    got = em.intersect(o, d, hints=hints)
+    assert got["err"][0] == 0, got["err"]
+    _same_hits(cs.intersect(o, d), got)
+
+
+def test_packed_tree_structure(pair):
+    """Children sit side by side, every leaf record's ref range is inside
+    leaf_refs, and every rope names a node of the tree (the smallest one that
+    covers that face, Popov et al. 2007) or -1 on the scene boundary."""
+    cs, em = pair
+    c = em.counts()
+    meta, split, leaves = em.tree()
+    tag = meta >> 30
+    child = (meta & 0x3FFFFFFF).astype(np.int64)
+    inner = tag != 3
+    assert (child[inner] + 1 < c["nodes"]).all()
+    assert (child[inner] > np.flatnonzero(inner)).all()
+    lf = child[~inner]
+    assert ((lf >= 0) & (lf < c["leaves"])).all()
+    assert len(np.unique(lf)) == c["leaves"]
+    first, count = leaves[:, 3], leaves[:, 7]
+    assert ((first >= 0) & (count >= 0) & (first + count <= c["refs"])).all()
+    ropes = leaves[:, 8:14]
+    assert ((ropes == -1) | ((ropes > 0) & (ropes < c["nodes"]))).all()
+    assert (ropes >= 0).any()
+
+
+def test_shade_and_next_dir_match_oracle(pair):
+    cs, em = pair
+    o, d = S.random_rays(4000, seed=13)
+    hit = cs.intersect(o, d)
+    m = hit["tri"] >= 0
+    o, d = o[m], d[m]
+    rng = np.random.default_rng(1)
+    strength = rng.uniform(0.1, 1.0, size=(len(o), 3)).astype(np.float32)
+    seeds = rng.integers(0, 2 ** 48, size=len(o), dtype=np.int64)
+    for dd in (0, 1):
+        ref = cs.shade(o, d, strength, hit["tri"][m], hit["t"][m], seeds, disable_diffuse=dd)
+        got = em.shade(o, d, strength, hit["tri"][m], hit["t"][m], seeds.view(np.uint64),
+                       disable_diffuse=dd)
+        for k in ("contrib", "hit_p", "normal", "strength", "param", "branch"):
+            assert np.array_equal(np.asarray(ref[k]).view(np.int32),
+                                  np.asarray(got[k]).view(np.int32)), k
+        assert np.array_equal(ref["seeds"].view(np.uint64), got["seeds"])
+        nref = cs.next_dir(ref["branch"], d, ref["hit_p"], ref["normal"], ref["strength"],
+                           ref["param"], ref["seeds"])
+        ngot = em.next_dir(got["branch"], d, got["hit_p"], got["normal"], got["strength"],
+                           got["param"], got["seeds"])
+        alive = nref["alive"] != 0
+        assert np.array_equal(nref["alive"], ngot["alive"])
+        for k in ("origins", "directions", "strength"):
+            assert np.array_equal(nref[k][alive].view(np.int32), ngot[k][alive].view(np.int32)), k
