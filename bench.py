@@ -147,6 +147,20 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def profiled_traffic():
+    """DRAM bytes (read + write) of one k_isect launch of this workload, from
+    the committed ncu summary (None when the summary is absent)."""
+    path = os.path.join(ROOT, "profiles", "k_isect_spheres64_512x512_spp64_d8.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return int(line.split(":")[1])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def make_scene():
     import hptracing_b200 as H
     from tests import scenes as S
@@ -297,7 +311,9 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "k_isect", "achieved": achieved,
                          "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
-                         "peak_kind": peak_kind, "traffic": None,
+                         "peak_kind": peak_kind,
+                         "traffic": profiled_traffic() if WORKLOAD.startswith("spheres64") else None,
+                         "traffic_source": "ncu --set full, one full-queue launch (profiles/)",
                          "algorithmic_bytes_per_launch": ib / max(1, isect_launches),
                          "launches": isect_launches,
                          "avg_launch_ms": isect_ms / max(1, isect_launches)},

@@ -6,6 +6,11 @@ Every CUDA and host C++ source under csrc/ is compiled in parallel into
 _build/ and linked into hptracing_b200/libhpt.so. Float contraction is off
 everywhere (-fmad=false for device code, -ffp-contract=off for host code):
 the kernels reproduce the reference's FP32 operation order bit for bit.
+
+The device index guards (HPT_DEVICE_CHECKS, csrc/checks.cuh) are part of
+the library: every index a kernel dereferences is range-checked, and a
+failing check is returned as an error status naming its site instead of
+touching memory.
 """
 import concurrent.futures
 import os
@@ -21,7 +26,7 @@ CLI = os.path.join(HERE, "hptracing")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
-          "-I", os.path.join(HERE, "..", "include")]
+          "-DHPT_DEVICE_CHECKS", "-I", os.path.join(HERE, "..", "include")]
 CUDA_FLAGS = ARCH + ["-lineinfo", "-fmad=false", "--expt-relaxed-constexpr", "-Xptxas", "-O3"]
 
 
@@ -103,23 +108,6 @@ def build(verbose=False, force=False):
         raise RuntimeError("link failed\n%s%s" % (r.stdout, r.stderr))
     build_cli(verbose)
     return LIB
-
-
-def build_checked(verbose=False):
-    """libhpt_check.so: the same sources with every device index range-checked
-    (-DHPT_DEVICE_CHECKS); a failing check is reported as an error status
-    naming its site instead of touching memory. For diagnosis only."""
-    bdir = os.path.join(HERE, "_build_check")
-    os.makedirs(bdir, exist_ok=True)
-    out = os.path.join(HERE, "libhpt_check.so")
-    srcs = _sources()
-    with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose, bdir, ["-DHPT_DEVICE_CHECKS"]), srcs))
-    cmd = [nvcc()] + ARCH + ["-shared", "-o", out] + objs + ["-lcudart", "-lpthread"]
-    r = subprocess.run(cmd, capture_output=True, text=True)
-    if r.returncode != 0:
-        raise RuntimeError("link failed\n%s%s" % (r.stdout, r.stderr))
-    return out
 
 
 if __name__ == "__main__":

@@ -1,7 +1,9 @@
-// Optional device self-checks. Built with -DHPT_DEVICE_CHECKS, every index
-// the kernels dereference is range-checked first; a failing check records
-// its site and value in the error word (first failure wins) and the access
-// is skipped. Normal builds compile the checks away.
+// Device index guards. The library is built with -DHPT_DEVICE_CHECKS: every
+// index a kernel dereferences is range-checked first; a failing check
+// records its site and value in the error word (first failure wins), the
+// access is skipped, and the host call returns HPT_ERR_INVALID_SCENE naming
+// the site. Compiling without the define removes the guards (experiments
+// only: that configuration is not shipped).
 #pragma once
 
 #include "device_types.h"

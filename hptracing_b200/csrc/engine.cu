@@ -128,6 +128,9 @@ __device__ __forceinline__ void flush_counts(DevCtrl* c, unsigned long long q, T
     n.repeats += __shfl_down_sync(kFull, n.repeats, o);
   }
   if ((threadIdx.x & 31) == 0 && q) {
+#ifdef HPT_DEVICE_CHECKS
+    atomicAdd(&c->chk_isect_done, (int)q);
+#endif
     atomicAdd(&c->isect_queries, q);
     atomicAdd(&c->nodes_visited, n.nodes);
     atomicAdd(&c->leaves_visited, n.leaves);
@@ -214,9 +217,6 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
             trav_init(J.scene, Ray{mk(J.view_p[0], J.view_p[1], J.view_p[2]), d}, st);
             active = true;
             ++queries;
-#ifdef HPT_DEVICE_CHECKS
-            atomicAdd(&c->chk_isect_done, 1);
-#endif
           }
         }
       }
@@ -450,9 +450,6 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
                         __float_as_int(P.R_r[i].w));
               active = true;
               ++queries;
-#ifdef HPT_DEVICE_CHECKS
-              atomicAdd(&c->chk_isect_done, 1);
-#endif
             }
           }
         }
@@ -626,11 +623,11 @@ void cuda_soft_fail(cudaError_t e, const char* what) {
 hpt_tuning default_tuning() {
   hpt_tuning t;
   memset(&t, 0, sizeof t);
-  t.capacity = 1 << 21;
+  t.capacity = 1 << 22;
   t.isect_block = 128;
   t.isect_min_blocks = 5;
   t.shade_block = 256;
-  t.refill_chunk = 16;
+  t.refill_chunk = 4;
   t.smem_nodes = 2048;
   t.use_graph = 0;
   return t;
@@ -671,6 +668,19 @@ hpt_status Engine::init() {
   HPT_CUDA(cudaMalloc(&ctrl_, sizeof(DevCtrl)));
   HPT_CUDA(cudaMallocHost(&ctrl_host_, sizeof(DevCtrl)));
   for (auto& e : ev_) HPT_CUDA(cudaEventCreate(&e));
+  for (auto& e : ev_done_) HPT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  HPT_CUDA(cudaMallocHost(&done_host_, 2 * sizeof(int32_t)));
+  // Per-job buffers come from the engine's own stream-ordered pool, which
+  // keeps up to 4 GiB of freed memory mapped between renders instead of
+  // returning it to the driver at every synchronisation.
+  cudaMemPoolProps props;
+  memset(&props, 0, sizeof props);
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  HPT_CUDA(cudaMemPoolCreate(&pool_, &props));
+  uint64_t keep = 4ull << 30;
+  HPT_CUDA(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
   return HPT_OK;
 }
 
@@ -703,6 +713,11 @@ Engine::~Engine() {
   HPT_SOFT(cudaFreeHost(host_jobs_));
   for (auto& e : ev_)
     if (e) HPT_SOFT(cudaEventDestroy(e));
+  for (auto& e : ev_done_)
+    if (e) HPT_SOFT(cudaEventDestroy(e));
+  for (auto& e : pev_) HPT_SOFT(cudaEventDestroy(e));
+  if (done_host_) HPT_SOFT(cudaFreeHost(done_host_));
+  if (pool_) HPT_SOFT(cudaMemPoolDestroy(pool_));
   if (stream) HPT_SOFT(cudaStreamDestroy(stream));
 }
 
@@ -831,12 +846,15 @@ hpt_status Engine::alloc_job(const JobSpec& js, bool want_accum, JobBuffers& b) 
   const hpt_render_params& p = js.params;
   const int64_t nx = (int64_t)p.sample_x * p.supersample_x, ny = (int64_t)p.sample_y * p.supersample_y;
   b.rays = nx * ny;
-  HPT_CUDA(cudaMallocAsync(&b.accum, (size_t)b.rays * 3 * sizeof(unsigned long long), stream));
-  HPT_CUDA(cudaMallocAsync(&b.flags, (size_t)b.rays * sizeof(uint32_t), stream));
-  HPT_CUDA(cudaMallocAsync(&b.prim, (size_t)b.rays * 8 * sizeof(float), stream));
-  HPT_CUDA(cudaMallocAsync(&b.prim_count, sizeof(int32_t), stream));
-  HPT_CUDA(cudaMallocAsync(&b.rgba, (size_t)p.sample_x * p.sample_y * 4, stream));
-  if (want_accum) HPT_CUDA(cudaMallocAsync(&b.accum_f, (size_t)b.rays * 3 * sizeof(float), stream));
+  auto take = [&](auto** ptr, size_t bytes) {
+    return cudaMallocFromPoolAsync(reinterpret_cast<void**>(ptr), bytes, pool_, stream);
+  };
+  HPT_CUDA(take(&b.accum, (size_t)b.rays * 3 * sizeof(unsigned long long)));
+  HPT_CUDA(take(&b.flags, (size_t)b.rays * sizeof(uint32_t)));
+  HPT_CUDA(take(&b.prim, (size_t)b.rays * 8 * sizeof(float)));
+  HPT_CUDA(take(&b.prim_count, sizeof(int32_t)));
+  HPT_CUDA(take(&b.rgba, (size_t)p.sample_x * p.sample_y * 4));
+  if (want_accum) HPT_CUDA(take(&b.accum_f, (size_t)b.rays * 3 * sizeof(float)));
   HPT_CUDA(cudaMemsetAsync(b.accum, 0, (size_t)b.rays * 3 * sizeof(unsigned long long), stream));
   HPT_CUDA(cudaMemsetAsync(b.flags, 0, (size_t)b.rays * sizeof(uint32_t), stream));
   HPT_CUDA(cudaMemsetAsync(b.prim_count, 0, sizeof(int32_t), stream));
@@ -1056,16 +1074,13 @@ hpt_status Engine::run(const std::vector<JobSpec>& jobs, hpt_render_stats* stats
   // batch k+1 runs (extra iterations after completion are empty launches).
   const int kBatch = 4;
   const bool prof = tuning.profile != 0;
-  int32_t* done_host = nullptr;
-  HPT_CUDA(cudaMallocHost(&done_host, 2 * sizeof(int32_t)));
+  int32_t* done_host = done_host_;
   done_host[0] = done_host[1] = 0;
-  cudaEvent_t ev_done[2];
-  HPT_SOFT(cudaEventCreateWithFlags(&ev_done[0], cudaEventDisableTiming));
-  HPT_SOFT(cudaEventCreateWithFlags(&ev_done[1], cudaEventDisableTiming));
-  std::vector<cudaEvent_t> pev;
-  if (prof) {
+  cudaEvent_t* ev_done = ev_done_;
+  std::vector<cudaEvent_t>& pev = pev_;
+  if (prof && pev.empty()) {
     pev.resize(2 * kBatch * 3);
-    for (auto& e : pev) HPT_SOFT(cudaEventCreate(&e));
+    for (auto& e : pev) HPT_CUDA(cudaEventCreate(&e));
   }
   float ms_shade = 0.f, ms_isect = 0.f;
   auto harvest = [&](int sl) {
@@ -1125,10 +1140,6 @@ hpt_status Engine::run(const std::vector<JobSpec>& jobs, hpt_render_stats* stats
   for (auto& b : bufs) free_job(b);
   cudaError_t e = cudaStreamSynchronize(stream);
   if (prof) harvest(slot);
-  for (auto& ev : pev) HPT_SOFT(cudaEventDestroy(ev));
-  HPT_SOFT(cudaEventDestroy(ev_done[0]));
-  HPT_SOFT(cudaEventDestroy(ev_done[1]));
-  HPT_SOFT(cudaFreeHost(done_host));
   if (e != cudaSuccess) return cuda_fail(e, "render");
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "render launch");

@@ -111,6 +111,10 @@ class Engine {
   float4* R_s_ = nullptr;
   float4* R_r_ = nullptr;
   cudaEvent_t ev_[6];
+  cudaEvent_t ev_done_[2] = {nullptr, nullptr};
+  std::vector<cudaEvent_t> pev_;  // profiling events, created on first use
+  int32_t* done_host_ = nullptr;  // pinned drain flags (double-buffered)
+  cudaMemPool_t pool_ = nullptr;  // per-job buffers
   hpt_status init_status_ = HPT_OK;
   hpt_status init();
   int occ_isect_ = 1, occ_shade_ = 1;
