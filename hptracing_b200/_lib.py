@@ -134,6 +134,7 @@ SIGNATURES = {
     "hpt_shade": (i32, [vp, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp]),
     "hpt_next_dir": (i32, [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "hpt_compact": (i32, [vp, i32, vp, P(i32)]),
+    "hpt_compact_noalloc": (i32, [vp, i32, vp, vp, vp]),
     "hpt_resolve": (i32, [vp, i32, i32, i32, i32, i32, f32, vp]),
     "hpt_batch_create": (i32, [i32, P(vp)]),
     "hpt_batch_add": (i32, [vp, vp, P(Camera), P(RenderParams), vp, vp, P(i32)]),

@@ -763,3 +763,64 @@ hpt_status hpt_batch_tuning_set(hpt_batch* batch, const hpt_tuning* in) {
 void hpt_batch_destroy(hpt_batch* batch) { delete batch; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// hpt_compact_noalloc: the compaction kernels over caller-owned device
+// buffers, with the per-block counts in a static device array instead of a
+// cudaMalloc'd one. For callers that cannot allocate device memory where
+// they call it (allocation synchronises the device and would stall their
+// stream; a fixed memory budget leaves nothing to allocate).
+// ---------------------------------------------------------------------------
+namespace {
+
+// One count per 2048-flag tile, plus one spare entry: 64 KB per device.
+constexpr int kNoallocMaxBlocks = HPT_COMPACT_NOALLOC_MAX_N / kCompactTile;
+static_assert(kNoallocMaxBlocks * kCompactTile == HPT_COMPACT_NOALLOC_MAX_N,
+              "the limit is a whole number of tiles");
+static __device__ __align__(256) int g_noalloc_block_counts[kNoallocMaxBlocks + 1];
+
+// Device address of g_noalloc_block_counts, looked up once per device with
+// that device current (the first call on a device does this set-up).
+hpt_status noalloc_scratch(int device, int** out) {
+  static std::mutex mu;
+  static std::vector<int*> addr;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)addr.size() <= device) addr.resize(device + 1, nullptr);
+  if (!addr[device]) {
+    void* p = nullptr;
+    HPT_CUDA(cudaGetSymbolAddress(&p, g_noalloc_block_counts));
+    addr[device] = static_cast<int*>(p);
+  }
+  *out = addr[device];
+  return HPT_OK;
+}
+
+}  // namespace
+
+extern "C" hpt_status hpt_compact_noalloc(const uint32_t* flags, int32_t n, int32_t* out,
+                                          int32_t* count, void* stream) {
+  if (n < 0 || !count || (n > 0 && (!flags || !out)))
+    return fail(HPT_ERR_INVALID_ARGUMENT, "bad compact arguments");
+  if (n > HPT_COMPACT_NOALLOC_MAX_N)
+    return fail(HPT_ERR_INVALID_ARGUMENT,
+                "hpt_compact_noalloc: n = %d exceeds the limit of %d flags (static scratch)", n,
+                HPT_COMPACT_NOALLOC_MAX_N);
+  int device = 0;
+  HPT_CUDA(cudaGetDevice(&device));
+  int* scratch = nullptr;
+  hpt_status s = noalloc_scratch(device, &scratch);
+  if (s != HPT_OK) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (n == 0) {
+    HPT_CUDA(cudaMemsetAsync(count, 0, sizeof(int32_t), st));
+    return HPT_OK;
+  }
+  const int nb = blocks_for(n, kCompactTile);
+  // Every entry [0, nb) is written by the count pass before the scan reads
+  // it; the total goes straight to the caller's counter.
+  k_compact_count<<<nb, kCompactThreads, 0, st>>>(flags, n, scratch);
+  k_compact_scan<<<1, 1024, 0, st>>>(scratch, nb, count);
+  k_compact_scatter<<<nb, kCompactThreads, 0, st>>>(flags, n, scratch, out);
+  HPT_CUDA(cudaGetLastError());
+  return HPT_OK;
+}

@@ -327,6 +327,26 @@ hpt_status hpt_next_dir(hpt_scene* scene, int32_t n, const int32_t* branch,
 hpt_status hpt_compact(const uint32_t* flags, int32_t n, int32_t* out,
                        int32_t* count);
 
+/* No counterpart in the reference. hpt_compact on DEVICE buffers that
+ * allocates nothing: for callers that must not allocate device memory
+ * mid-stream - cudaMalloc/cudaFree synchronise the whole device, which
+ * would stall a stream-ordered pipeline, and a caller that has divided a
+ * fixed memory budget among its buffers has none left to give. flags,
+ * out and count are device pointers; the work is enqueued on `stream`
+ * (a cudaStream_t, NULL = legacy default stream) and the call returns
+ * without waiting: *count is valid once the stream reaches that point.
+ * The block-count scratch is a fixed static device array, so n is limited
+ * to HPT_COMPACT_NOALLOC_MAX_N flags (larger n: HPT_ERR_INVALID_ARGUMENT,
+ * nothing enqueued). The first call on each device looks up that array's
+ * address (set-up, with the device current); make that first call before
+ * any stream capture. Every call shares the one array: calls whose work
+ * overlaps on the GPU (different streams, or host threads) race on it and
+ * must be serialised by the caller. Each call overwrites every scratch
+ * entry it reads, so no state carries over between calls. */
+#define HPT_COMPACT_NOALLOC_MAX_N (16384 * 2048)
+hpt_status hpt_compact_noalloc(const uint32_t* flags, int32_t n,
+                               int32_t* out, int32_t* count, void* stream);
+
 /* get_image (src/hp/cl_src/kernel.cl:615-652) over a float accumulator of
  * (sample_x*ssx) x (sample_y*ssy) rays. */
 hpt_status hpt_resolve(const float* accum, int32_t sample_x,
