@@ -271,6 +271,14 @@ class Scene:
     def set_tuning(self, t):
         check(lib().hpt_tuning_set(self._h, C.byref(t)))
 
+    def autotune(self, camera, params, cache_path=None):
+        """Searches the tuning on a short render of (camera, params), keeps
+        the best in this scene and returns it (hpt_autotune)."""
+        t = Tuning()
+        path = cache_path.encode() if cache_path else None
+        check(lib().hpt_autotune(self._h, C.byref(camera), C.byref(params), path, C.byref(t)))
+        return t
+
     def render(self, camera, params, want_accum=False):
         rgba = np.zeros((params.sample_y, params.sample_x, 4), np.uint8)
         acc = None
@@ -420,7 +428,7 @@ class Batch:
 class Server:
     """Continuous-batching render server (hpt_server)."""
 
-    def __init__(self, device=0, max_jobs=64, memory_budget=8 << 30, capacity=1 << 21,
+    def __init__(self, device=0, max_jobs=64, memory_budget=8 << 30, capacity=1 << 22,
                  progressive=0):
         cfg = ServerConfig(device, max_jobs, memory_budget, capacity, progressive)
         h = C.c_void_p()
@@ -455,6 +463,11 @@ class Server:
 
     def pending(self):
         return lib().hpt_server_pending(self._h)
+
+    def stats(self):
+        s = RenderStats()
+        check(lib().hpt_server_stats_get(self._h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in RenderStats._fields_}
 
     def close(self):
         if getattr(self, "_h", None):

@@ -149,6 +149,7 @@ SIGNATURES = {
     "hpt_server_poll": (i32, [vp, u64, P(RequestInfo), vp, vp]),
     "hpt_server_cancel": (i32, [vp, u64]),
     "hpt_server_pending": (i32, [vp]),
+    "hpt_server_stats_get": (i32, [vp, P(RenderStats)]),
     "hpt_server_destroy": (None, [vp]),
     "hpt_autotune": (i32, [vp, P(Camera), P(RenderParams), C.c_char_p, P(Tuning)]),
 }

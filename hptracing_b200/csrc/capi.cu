@@ -14,10 +14,6 @@
 
 using namespace hpt;
 
-struct hpt_scene {
-  SceneHandle h;
-};
-
 namespace hpt {
 
 namespace {

@@ -107,6 +107,7 @@ struct DevSlot {
   int64_t num_paths;        // hits * spp, set after the primary pass
   int64_t cursor;
   unsigned long long done;  // paths finished (flushed)
+  unsigned long long queries;  // secondary intersect queries issued
   int32_t alloc;            // new paths granted for the coming shade pass
   int32_t active;           // admitted and not yet fully issued
 };

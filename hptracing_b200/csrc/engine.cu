@@ -118,6 +118,16 @@ __device__ __forceinline__ void count_done(DevSlot* slots, bool done, int slot) 
     atomicAdd(&slots[slot].done, (unsigned long long)__popc(same & m));
 }
 
+// Counts the paths each slot sends to the intersect queue (one atomic per
+// (warp, slot)).
+__device__ __forceinline__ void count_queries(DevSlot* slots, bool alive, int slot) {
+  const unsigned m = __ballot_sync(kFull, alive);
+  if (!m) return;
+  const unsigned same = __match_any_sync(kFull, alive ? slot : -1);
+  if (alive && (__ffs(same & m) - 1) == (int)(threadIdx.x & 31))
+    atomicAdd(&slots[slot].queries, (unsigned long long)__popc(same & m));
+}
+
 // Warp-level reduction of the per-lane query and work counters.
 __device__ __forceinline__ void flush_counts(DevCtrl* c, unsigned long long q, TravCount n) {
   for (int o = 16; o > 0; o >>= 1) {
@@ -261,6 +271,7 @@ __global__ void k_admit(EngineParams P) {
     S.num_paths = (int64_t)(*P.jobs[s].prim_count) * P.jobs[s].spp;
     S.cursor = 0;
     S.done = 0;
+    S.queries = 0;
     S.alloc = 0;
     S.active = 1;
   }
@@ -377,6 +388,7 @@ __global__ void __launch_bounds__(BS) k_shade(EngineParams P) {
       }
     }
     count_done(P.slots, ended, slot);
+    count_queries(P.slots, alive, slot);
     // Block-level stable compaction: ballot per warp, scan over warps.
     const unsigned m = __ballot_sync(kFull, alive);
     if (lane == 0) warp_counts[warp] = __popc(m);
@@ -562,10 +574,10 @@ __device__ __forceinline__ uint8_t to_unorm8(float x) {
   return (uint8_t)__float2int_rn(v);
 }
 
-// get_image (kernel.cl:615-652) from the fixed-point accumulators. spp is
-// the divisor (the full sample count, or the samples completed so far for a
-// progressive preview).
-__global__ void k_resolve(const DevJob* jp, int W, int H, int ssx, int ssy, int spp,
+// get_image (kernel.cl:615-652) from the fixed-point accumulators.
+// samples is the divisor: the full sample count for the final image, or the
+// samples completed so far for a progressive preview.
+__global__ void k_resolve(const DevJob* jp, int W, int H, int ssx, int ssy, float samples,
                           float brightness, uint8_t* rgba, float* accum_f) {
   const int gx = blockIdx.x * blockDim.x + threadIdx.x;
   const int gy = blockIdx.y * blockDim.y + threadIdx.y;
@@ -588,7 +600,7 @@ __global__ void k_resolve(const DevJob* jp, int W, int H, int ssx, int ssy, int 
       py = __fadd_rn(py, vy);
       pz = __fadd_rn(pz, vz);
     }
-  const float nss = (float)(ssx * ssy), ns = (float)spp;
+  const float nss = (float)(ssx * ssy), ns = samples;
   px = __fmul_rn(__fdiv_rn(__fdiv_rn(px, nss), ns), brightness);
   py = __fmul_rn(__fdiv_rn(__fdiv_rn(py, nss), ns), brightness);
   pz = __fmul_rn(__fdiv_rn(__fdiv_rn(pz, nss), ns), brightness);
@@ -711,6 +723,7 @@ Engine::~Engine() {
   HPT_SOFT(cudaFreeHost(host_i32_));
   HPT_SOFT(cudaFreeHost(host_i64_));
   HPT_SOFT(cudaFreeHost(host_jobs_));
+  HPT_SOFT(cudaFreeHost(slots_host_));
   for (auto& e : ev_)
     if (e) HPT_SOFT(cudaEventDestroy(e));
   for (auto& e : ev_done_)
@@ -718,6 +731,7 @@ Engine::~Engine() {
   for (auto& e : pev_) HPT_SOFT(cudaEventDestroy(e));
   if (done_host_) HPT_SOFT(cudaFreeHost(done_host_));
   if (pool_) HPT_SOFT(cudaMemPoolDestroy(pool_));
+  if (graph_exec_) HPT_SOFT(cudaGraphExecDestroy(graph_exec_));
   if (stream) HPT_SOFT(cudaStreamDestroy(stream));
 }
 
@@ -770,6 +784,8 @@ hpt_status Engine::ensure_slots(int slots) {
   HPT_SOFT(cudaFreeHost(host_i32_));
   HPT_SOFT(cudaFreeHost(host_i64_));
   HPT_SOFT(cudaFreeHost(host_jobs_));
+  HPT_SOFT(cudaFreeHost(slots_host_));
+  slots_host_ = nullptr;
   jobs_ = nullptr;
   slot_state_ = nullptr;
   order_ = quota_slot_ = quota_prefix_ = prim_slot_ = nullptr;
@@ -789,6 +805,7 @@ hpt_status Engine::ensure_slots(int slots) {
   HPT_CUDA(cudaMallocHost(&host_i32_, (2 * n + 3) * sizeof(int32_t)));
   HPT_CUDA(cudaMallocHost(&host_i64_, (n + 1) * sizeof(int64_t)));
   HPT_CUDA(cudaMallocHost(&host_jobs_, n * sizeof(DevJob)));
+  HPT_CUDA(cudaMallocHost(&slots_host_, n * sizeof(DevSlot)));
   HPT_CUDA(cudaMemsetAsync(jobs_, 0, n * sizeof(DevJob), stream));
   HPT_CUDA(cudaMemsetAsync(slot_state_, 0, n * sizeof(DevSlot), stream));
   HPT_CUDA(cudaMemsetAsync(quota_prefix_, 0, (n + 1) * sizeof(int32_t), stream));
@@ -1005,6 +1022,39 @@ hpt_status Engine::admit(const std::vector<int>& slot_ids, const std::vector<Dev
   return HPT_OK;
 }
 
+hpt_status Engine::ensure_graph(const DevScene* shared_scene, int iterations) {
+  const void* key_nodes = shared_scene ? (const void*)shared_scene->nodes : nullptr;
+  if (graph_exec_ && graph_nodes_ == key_nodes && graph_capacity_ == capacity_ &&
+      graph_slots_ == slots_ && graph_iters_ == iterations && graph_tuning_ == isect_variant() &&
+      graph_smem_ == tuning.smem_nodes && graph_refill_ == tuning.refill_chunk)
+    return HPT_OK;
+  if (graph_exec_) {
+    HPT_SOFT(cudaGraphExecDestroy(graph_exec_));
+    graph_exec_ = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  HPT_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  for (int k = 0; k < iterations; ++k) launch_iteration(shared_scene, nullptr);
+  const cudaError_t launch = cudaGetLastError();
+  const cudaError_t end = cudaStreamEndCapture(stream, &g);
+  if (launch != cudaSuccess) {
+    if (g) HPT_SOFT(cudaGraphDestroy(g));
+    return cuda_fail(launch, "graph capture");
+  }
+  HPT_CUDA(end);
+  const cudaError_t inst = cudaGraphInstantiate(&graph_exec_, g, 0);
+  HPT_SOFT(cudaGraphDestroy(g));
+  HPT_CUDA(inst);
+  graph_nodes_ = key_nodes;
+  graph_capacity_ = capacity_;
+  graph_slots_ = slots_;
+  graph_iters_ = iterations;
+  graph_tuning_ = isect_variant();
+  graph_smem_ = tuning.smem_nodes;
+  graph_refill_ = tuning.refill_chunk;
+  return HPT_OK;
+}
+
 void Engine::launch_iteration(const DevScene* shared_scene, cudaEvent_t* ev) {
   float4* A[8] = {A_o_[0], A_d_[0], A_s_[0], A_r_[0], A_o_[1], A_d_[1], A_s_[1], A_r_[1]};
   float4* R[4] = {R_o_, R_d_, R_s_, R_r_};
@@ -1021,11 +1071,29 @@ void Engine::launch_iteration(const DevScene* shared_scene, cudaEvent_t* ev) {
   k_ctrl<<<1, 1, 0, stream>>>(P);
 }
 
-void Engine::launch_resolve(int slot, const JobSpec& js, const JobBuffers& b) {
+void Engine::launch_resolve(int slot, const JobSpec& js, const JobBuffers& b, float samples) {
   const hpt_render_params& p = js.params;
   dim3 blk(16, 16), grd((p.sample_x + 15) / 16, (p.sample_y + 15) / 16);
   k_resolve<<<grd, blk, 0, stream>>>(jobs_ + slot, p.sample_x, p.sample_y, p.supersample_x,
-                                      p.supersample_y, p.sample, p.brightness, b.rgba, b.accum_f);
+                                      p.supersample_y, samples > 0.f ? samples : (float)p.sample,
+                                      p.brightness, b.rgba, b.accum_f);
+}
+
+hpt_status Engine::read_slots(std::vector<DevSlot>& out) {
+  out.resize(slots_);
+  if (slots_ == 0) return HPT_OK;
+  HPT_CUDA(cudaMemcpyAsync(slots_host_, slot_state_, (size_t)slots_ * sizeof(DevSlot),
+                           cudaMemcpyDeviceToHost, stream));
+  HPT_CUDA(cudaStreamSynchronize(stream));
+  std::copy(slots_host_, slots_host_ + slots_, out.begin());
+  return HPT_OK;
+}
+
+hpt_status Engine::read_ctrl(DevCtrl* out) {
+  HPT_CUDA(cudaMemcpyAsync(ctrl_host_, ctrl_, sizeof(DevCtrl), cudaMemcpyDeviceToHost, stream));
+  HPT_CUDA(cudaStreamSynchronize(stream));
+  *out = *ctrl_host_;
+  return HPT_OK;
 }
 
 hpt_status Engine::run(const std::vector<JobSpec>& jobs, hpt_render_stats* stats) {
@@ -1105,13 +1173,30 @@ hpt_status Engine::run(const std::vector<JobSpec>& jobs, hpt_render_stats* stats
     max_depth = std::max(max_depth, p.depth);
   }
   const int64_t max_batches = (2 * (work / std::max(1, capacity_) + max_depth) + 64) / kBatch + 4;
+  // With use_graph, the kBatch iterations are replayed from one CUDA graph
+  // (their parameters live in device memory, so one capture serves every
+  // batch); it is captured again when the queues, the slot table or the
+  // shared-scene prefix change. Profiling needs per-kernel events: eager.
+  const bool use_graph = tuning.use_graph != 0 && !prof;
+  if (use_graph) {
+    s = ensure_graph(shared_dev, kBatch);
+    if (s != HPT_OK) {
+      for (auto& b : bufs) free_job(b);
+      HPT_SOFT(cudaStreamSynchronize(stream));
+      return s;
+    }
+  }
   int64_t guard = 0;
   bool drained = false;
   int slot = 0;
   bool pending = false;
   while (true) {
-    for (int k = 0; k < kBatch; ++k)
-      launch_iteration(shared_dev, prof ? &pev[(slot * kBatch + k) * 3] : nullptr);
+    if (use_graph) {
+      HPT_CUDA(cudaGraphLaunch(graph_exec_, stream));
+    } else {
+      for (int k = 0; k < kBatch; ++k)
+        launch_iteration(shared_dev, prof ? &pev[(slot * kBatch + k) * 3] : nullptr);
+    }
     HPT_SOFT(cudaMemcpyAsync(&done_host[slot], &ctrl_->done, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
     HPT_SOFT(cudaEventRecord(ev_done[slot], stream));
     if (pending) {

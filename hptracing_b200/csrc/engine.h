@@ -78,7 +78,14 @@ class Engine {
                    const DevScene* shared_scene);
   hpt_status set_order(const std::vector<int>& order);
   void launch_iteration(const DevScene* shared_scene, cudaEvent_t* ev3 = nullptr);
-  void launch_resolve(int slot, const JobSpec& js, const JobBuffers& b);
+  // Captures `iterations` consecutive iterations into graph_exec_ (kept
+  // until the queues, slots, shared scene or tuning change).
+  hpt_status ensure_graph(const DevScene* shared_scene, int iterations);
+  // samples: the divisor of the accumulated radiance (<= 0: params.sample).
+  void launch_resolve(int slot, const JobSpec& js, const JobBuffers& b, float samples = 0.f);
+  // Synchronous read-back of the slot table / control block.
+  hpt_status read_slots(std::vector<DevSlot>& out);
+  hpt_status read_ctrl(DevCtrl* out);
   void reset_ctrl();
   DevCtrl* ctrl_dev() const { return ctrl_; }
   DevSlot* slots_dev() const { return slot_state_; }
@@ -99,6 +106,7 @@ class Engine {
   int32_t* host_i32_ = nullptr;   // pinned staging for small uploads
   int64_t* host_i64_ = nullptr;
   DevJob* host_jobs_ = nullptr;
+  DevSlot* slots_host_ = nullptr;  // pinned mirror for read_slots
   // Shade queues (double-buffered) and the intersect queue.
   float4* A_o_[2] = {nullptr, nullptr};
   float4* A_d_[2] = {nullptr, nullptr};
@@ -115,6 +123,10 @@ class Engine {
   std::vector<cudaEvent_t> pev_;  // profiling events, created on first use
   int32_t* done_host_ = nullptr;  // pinned drain flags (double-buffered)
   cudaMemPool_t pool_ = nullptr;  // per-job buffers
+  cudaGraphExec_t graph_exec_ = nullptr;
+  const void* graph_nodes_ = nullptr;
+  int graph_capacity_ = 0, graph_slots_ = 0, graph_iters_ = 0, graph_tuning_ = -1;
+  int graph_smem_ = -1, graph_refill_ = -1;
   hpt_status init_status_ = HPT_OK;
   hpt_status init();
   int occ_isect_ = 1, occ_shade_ = 1;
@@ -155,3 +167,8 @@ void cuda_soft_fail(cudaError_t e, const char* what);
   } while (0)
 
 }  // namespace hpt
+
+// The opaque scene handle of the C ABI.
+struct hpt_scene {
+  hpt::SceneHandle h;
+};

@@ -1,35 +1,508 @@
-// Serving loop and autotuner (filled in below the render path).
+// Serving loop and autotuner. Neither has a reference counterpart: the
+// reference re-runs TraceRunner::run for every camera move of its GLUT loop
+// (src/hptracing.cpp:124-211), one frame at a time.
+//
+// Serving is continuous batching over the engine's job slots: requests
+// against device-resident scenes wait in a queue, are admitted as soon as a
+// slot and their device footprint (ray state, accumulators, image) fit,
+// share one wavefront with every request already running (smallest
+// remaining work first), and are resolved and copied back the pump after
+// their last path finishes. Random streams are keyed by (request seed, ray,
+// sample, bounce) and radiance is summed in fixed point, so a request's
+// image is bit-identical whether it runs alone or in any mix.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
 #include "../../include/hpt.h"
 #include "engine.h"
 
 using namespace hpt;
 
-struct hpt_server {
-  int dummy;
+namespace {
+
+enum RequestState { kQueued = 0, kRunning = 1, kDone = 2, kFailed = 3, kCancelled = 4 };
+
+struct Request {
+  uint64_t id = 0;
+  JobSpec js;
+  int state = kQueued;
+  int slot = -1;
+  bool want_accum = true;
+  bool cancel = false;
+  JobBuffers buf;
+  int64_t footprint = 0;
+  int64_t rays = 0;
+  int64_t paths = -1;       // hits * spp, known after the primary pass
+  int64_t done_paths = 0;
+  int64_t queries = 0;
+  double submit_ms = 0, admit_ms = 0, done_ms = 0;
+  hpt_status error = HPT_OK;
+  std::vector<uint8_t> rgba;
+  std::vector<float> accum;
 };
+
+}  // namespace
+
+struct hpt_server {
+  hpt_server_config cfg{};
+  std::unique_ptr<Engine> engine;
+  std::vector<hpt_scene*> scenes;
+  std::mutex mu;
+  std::map<uint64_t, std::unique_ptr<Request>> reqs;
+  std::deque<uint64_t> queue;
+  std::vector<uint64_t> slot_req;  // slot -> running request id, 0 = free
+  int64_t used_bytes = 0;
+  uint64_t next_id = 1;
+  std::chrono::steady_clock::time_point t0;
+  std::vector<DevSlot> slot_view;
+  int64_t completed = 0;
+  int64_t pumps = 0;
+
+  double now_ms() const {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+        .count();
+  }
+  Request* find(uint64_t id) {
+    auto it = reqs.find(id);
+    return it == reqs.end() ? nullptr : it->second.get();
+  }
+  // Active slots, smallest remaining work first.
+  std::vector<int> order() const {
+    std::vector<std::pair<int64_t, int>> v;
+    for (size_t k = 0; k < slot_req.size(); ++k) {
+      if (!slot_req[k]) continue;
+      const Request* r = reqs.at(slot_req[k]).get();
+      const int64_t total = r->paths >= 0 ? r->paths : r->rays * r->js.params.sample;
+      v.push_back({total - r->done_paths, (int)k});
+    }
+    std::stable_sort(v.begin(), v.end());
+    std::vector<int> o;
+    for (auto& p : v) o.push_back(p.second);
+    return o;
+  }
+  hpt_status admit_pending();
+  hpt_status collect();
+};
+
+// Moves queued requests into free slots while the memory budget allows
+// (first fit in arrival order), then runs their primary pass.
+hpt_status hpt_server::admit_pending() {
+  std::vector<int> ids;
+  std::vector<DevJob> jobs;
+  std::vector<int64_t> rays;
+  for (auto it = queue.begin(); it != queue.end();) {
+    Request* r = find(*it);
+    if (!r || r->cancel) {
+      if (r) r->state = kCancelled;
+      it = queue.erase(it);
+      continue;
+    }
+    int slot = -1;
+    for (size_t k = 0; k < slot_req.size(); ++k)
+      if (!slot_req[k]) {
+        slot = (int)k;
+        break;
+      }
+    if (slot < 0) break;
+    if (used_bytes + r->footprint > cfg.memory_budget) {
+      ++it;
+      continue;
+    }
+    hpt_status s = engine->alloc_job(r->js, r->want_accum, r->buf);
+    if (s == HPT_ERR_OUT_OF_MEMORY) {
+      engine->free_job(r->buf);
+      break;  // retry after something finishes
+    }
+    if (s != HPT_OK) return s;
+    r->slot = slot;
+    r->state = kRunning;
+    r->admit_ms = now_ms();
+    slot_req[slot] = r->id;
+    used_bytes += r->footprint;
+    ids.push_back(slot);
+    jobs.push_back(engine->make_job(r->js, r->buf));
+    rays.push_back(r->rays);
+    it = queue.erase(it);
+  }
+  if (ids.empty()) return HPT_OK;
+  return engine->admit(ids, jobs, rays, order(), nullptr);
+}
+
+// Reads the slot table; resolves, copies back and releases every request
+// whose paths have all finished.
+hpt_status hpt_server::collect() {
+  hpt_status s = engine->read_slots(slot_view);
+  if (s != HPT_OK) return s;
+  std::vector<Request*> finished;
+  for (size_t k = 0; k < slot_req.size(); ++k) {
+    if (!slot_req[k]) continue;
+    Request* r = reqs.at(slot_req[k]).get();
+    const DevSlot& S = slot_view[k];
+    r->paths = S.num_paths;
+    r->done_paths = (int64_t)S.done;
+    r->queries = r->rays + (int64_t)S.queries;
+    if ((int64_t)S.done >= S.num_paths && S.cursor >= S.num_paths) finished.push_back(r);
+  }
+  if (finished.empty()) return HPT_OK;
+  for (Request* r : finished) {
+    const hpt_render_params& p = r->js.params;
+    engine->launch_resolve(r->slot, r->js, r->buf);
+    r->rgba.resize((size_t)p.sample_x * p.sample_y * 4);
+    HPT_CUDA(cudaMemcpyAsync(r->rgba.data(), r->buf.rgba, r->rgba.size(), cudaMemcpyDeviceToHost,
+                             engine->stream));
+    if (r->want_accum) {
+      r->accum.resize((size_t)r->rays * 3);
+      HPT_CUDA(cudaMemcpyAsync(r->accum.data(), r->buf.accum_f, r->accum.size() * sizeof(float),
+                               cudaMemcpyDeviceToHost, engine->stream));
+    }
+  }
+  HPT_CUDA(cudaStreamSynchronize(engine->stream));
+  const double t = now_ms();
+  for (Request* r : finished) {
+    engine->free_job(r->buf);
+    slot_req[r->slot] = 0;
+    used_bytes -= r->footprint;
+    r->slot = -1;
+    r->state = r->cancel ? kCancelled : kDone;
+    r->done_ms = t;
+    ++completed;
+  }
+  return engine->set_order(order());
+}
 
 extern "C" {
 
-hpt_status hpt_server_create(const hpt_server_config*, hpt_server** out) {
-  if (out) *out = nullptr;
-  return fail(HPT_ERR_UNSUPPORTED, "server not built yet");
+hpt_status hpt_server_create(const hpt_server_config* config, hpt_server** out) {
+  if (!config || !out) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  if (config->max_jobs < 1 || config->max_jobs > 4096 || config->memory_budget <= 0 ||
+      config->capacity < 1024 || config->capacity > (1 << 27))
+    return fail(HPT_ERR_INVALID_ARGUMENT, "server config out of range");
+  if (config->device < 0 || config->device >= hpt_device_count())
+    return fail(HPT_ERR_CUDA, "no CUDA device %d", config->device);
+  try {
+    std::unique_ptr<hpt_server> s(new hpt_server());
+    s->cfg = *config;
+    s->t0 = std::chrono::steady_clock::now();
+    s->engine.reset(new Engine(config->device));
+    s->engine->tuning.capacity = config->capacity;
+    s->engine->tuning.smem_nodes = 0;  // requests mix scenes
+    HPT_CUDA(cudaSetDevice(config->device));
+    hpt_status st = s->engine->ensure_capacity(config->capacity);
+    if (st == HPT_OK) st = s->engine->ensure_slots(config->max_jobs);
+    if (st != HPT_OK) return st;
+    s->engine->reset_ctrl();
+    HPT_CUDA(cudaStreamSynchronize(s->engine->stream));
+    s->slot_req.assign(config->max_jobs, 0);
+    *out = s.release();
+    return HPT_OK;
+  } catch (const std::bad_alloc&) {
+    return fail(HPT_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
 }
-hpt_status hpt_server_add_scene(hpt_server*, hpt_scene*, int32_t*) {
-  return fail(HPT_ERR_UNSUPPORTED, "server not built yet");
+
+hpt_status hpt_server_add_scene(hpt_server* server, hpt_scene* scene, int32_t* scene_slot) {
+  if (!server || !scene || !scene_slot) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  std::lock_guard<std::mutex> lk(server->mu);
+  if (scene->h.scene.device != server->cfg.device)
+    return fail(HPT_ERR_INVALID_ARGUMENT, "scene lives on another device");
+  server->scenes.push_back(scene);
+  *scene_slot = (int32_t)server->scenes.size() - 1;
+  return HPT_OK;
 }
-hpt_status hpt_server_submit(hpt_server*, int32_t, const hpt_camera*, const hpt_render_params*,
-                             uint64_t*) {
-  return fail(HPT_ERR_UNSUPPORTED, "server not built yet");
+
+hpt_status hpt_server_submit(hpt_server* server, int32_t scene_slot, const hpt_camera* camera,
+                             const hpt_render_params* params, uint64_t* request_id) {
+  if (!server || !request_id) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  hpt_status s = check_render_params(camera, params);
+  if (s != HPT_OK) return s;
+  std::lock_guard<std::mutex> lk(server->mu);
+  if (scene_slot < 0 || scene_slot >= (int32_t)server->scenes.size())
+    return fail(HPT_ERR_NOT_FOUND, "scene slot %d not registered", scene_slot);
+  std::unique_ptr<Request> r(new Request());
+  r->id = server->next_id++;
+  r->js.scene = &server->scenes[scene_slot]->h.scene;
+  r->js.camera = *camera;
+  r->js.params = *params;
+  r->rays = (int64_t)params->sample_x * params->supersample_x * params->sample_y *
+            params->supersample_y;
+  r->footprint = job_footprint(*params, r->want_accum);
+  if (r->footprint > server->cfg.memory_budget)
+    return fail(HPT_ERR_OUT_OF_MEMORY, "request needs %lld bytes, budget is %lld",
+                (long long)r->footprint, (long long)server->cfg.memory_budget);
+  r->submit_ms = server->now_ms();
+  *request_id = r->id;
+  server->queue.push_back(r->id);
+  server->reqs[r->id] = std::move(r);
+  return HPT_OK;
 }
-hpt_status hpt_server_pump(hpt_server*, int32_t) { return fail(HPT_ERR_UNSUPPORTED, "server not built yet"); }
-hpt_status hpt_server_poll(hpt_server*, uint64_t, hpt_request_info*, uint8_t*, float*) {
-  return fail(HPT_ERR_UNSUPPORTED, "server not built yet");
+
+hpt_status hpt_server_pump(hpt_server* server, int32_t max_iterations) {
+  if (!server) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  std::lock_guard<std::mutex> lk(server->mu);
+  HPT_CUDA(cudaSetDevice(server->cfg.device));
+  hpt_status s = server->admit_pending();
+  if (s != HPT_OK) return s;
+  bool running = false;
+  for (uint64_t id : server->slot_req) running = running || id != 0;
+  if (!running) return HPT_OK;
+  for (int i = 0; i < std::max(1, max_iterations); ++i) server->engine->launch_iteration(nullptr);
+  HPT_CUDA(cudaGetLastError());
+  ++server->pumps;
+  s = server->collect();
+  if (s != HPT_OK) return s;
+  DevCtrl c;
+  s = server->engine->read_ctrl(&c);
+  if (s != HPT_OK) return s;
+  if (c.err.flags & 2u)
+    return fail(HPT_ERR_INVALID_SCENE, "device self-check %d failed (value %lld)", c.err.site,
+                (long long)c.err.value);
+  if (c.err.flags & 1u) return fail(HPT_ERR_TRAVERSAL_LIMIT, "a traversal hit its step cap");
+  return HPT_OK;
 }
-hpt_status hpt_server_cancel(hpt_server*, uint64_t) { return fail(HPT_ERR_UNSUPPORTED, "server not built yet"); }
-int32_t hpt_server_pending(const hpt_server*) { return 0; }
-void hpt_server_destroy(hpt_server* s) { delete s; }
-hpt_status hpt_autotune(hpt_scene*, const hpt_camera*, const hpt_render_params*, const char*,
-                        hpt_tuning*) {
-  return fail(HPT_ERR_UNSUPPORTED, "autotune not built yet");
+
+hpt_status hpt_server_poll(hpt_server* server, uint64_t request_id, hpt_request_info* info,
+                           uint8_t* rgba_out, float* accum_out) {
+  if (!server) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  std::lock_guard<std::mutex> lk(server->mu);
+  Request* r = server->find(request_id);
+  if (!r) return fail(HPT_ERR_NOT_FOUND, "unknown request %llu", (unsigned long long)request_id);
+  const hpt_render_params& p = r->js.params;
+  const int64_t per_sample = r->paths > 0 ? r->paths / std::max(1, p.sample) : 0;
+  if (info) {
+    info->state = r->state;
+    info->samples_done = r->state == kDone ? p.sample
+                         : per_sample > 0  ? (int32_t)(r->done_paths / per_sample)
+                                           : 0;
+    info->submit_ms = r->submit_ms;
+    info->admit_ms = r->admit_ms;
+    info->done_ms = r->done_ms;
+    info->intersect_queries = r->queries;
+  }
+  if (r->state == kDone) {
+    if (rgba_out) std::memcpy(rgba_out, r->rgba.data(), r->rgba.size());
+    if (accum_out && r->want_accum)
+      std::memcpy(accum_out, r->accum.data(), r->accum.size() * sizeof(float));
+    server->reqs.erase(request_id);
+    return HPT_OK;
+  }
+  if (r->state == kCancelled || r->state == kFailed) {
+    const hpt_status e = r->state == kCancelled ? HPT_ERR_CANCELLED : r->error;
+    server->reqs.erase(request_id);
+    return fail(e, "request %llu %s", (unsigned long long)request_id,
+                e == HPT_ERR_CANCELLED ? "was cancelled" : "failed");
+  }
+  // Running: a progressive preview divides by the samples completed so far
+  // (paths finish out of order, so this is the fraction of finished paths).
+  if (r->state == kRunning && server->cfg.progressive && rgba_out && per_sample > 0 &&
+      r->done_paths > 0) {
+    const float samples = (float)((double)r->done_paths / (double)per_sample);
+    server->engine->launch_resolve(r->slot, r->js, r->buf, samples);
+    HPT_CUDA(cudaMemcpyAsync(rgba_out, r->buf.rgba, (size_t)p.sample_x * p.sample_y * 4,
+                             cudaMemcpyDeviceToHost, server->engine->stream));
+    HPT_CUDA(cudaStreamSynchronize(server->engine->stream));
+  }
+  return HPT_ERR_BUSY;
 }
+
+hpt_status hpt_server_cancel(hpt_server* server, uint64_t request_id) {
+  if (!server) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  std::lock_guard<std::mutex> lk(server->mu);
+  Request* r = server->find(request_id);
+  if (!r) return fail(HPT_ERR_NOT_FOUND, "unknown request %llu", (unsigned long long)request_id);
+  r->cancel = true;  // queued: dropped at the next admission; running: discarded when done
+  if (r->state == kQueued) r->state = kCancelled;
+  return HPT_OK;
+}
+
+int32_t hpt_server_pending(const hpt_server* server) {
+  if (!server) return 0;
+  hpt_server* s = const_cast<hpt_server*>(server);
+  std::lock_guard<std::mutex> lk(s->mu);
+  int32_t n = 0;
+  for (auto& kv : s->reqs) n += kv.second->state == kQueued || kv.second->state == kRunning;
+  return n;
+}
+
+hpt_status hpt_server_stats_get(hpt_server* server, hpt_render_stats* out) {
+  if (!server || !out) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
+  std::lock_guard<std::mutex> lk(server->mu);
+  DevCtrl c;
+  hpt_status s = server->engine->read_ctrl(&c);
+  if (s != HPT_OK) return s;
+  memset(out, 0, sizeof *out);
+  out->intersect_queries = (int64_t)c.isect_queries;
+  out->shade_calls = (int64_t)c.shades;
+  out->iterations = (int32_t)c.iterations;
+  out->error_flags = (int32_t)c.err.flags;
+  out->nodes_visited = (int64_t)c.nodes_visited;
+  out->leaves_visited = (int64_t)c.leaves_visited;
+  out->triangle_tests = (int64_t)c.tri_tests;
+  out->triangle_repeats = (int64_t)c.tri_repeats;
+  out->paths = server->completed;
+  return HPT_OK;
+}
+
+void hpt_server_destroy(hpt_server* server) {
+  if (!server) return;
+  {
+    std::lock_guard<std::mutex> lk(server->mu);
+    if (server->engine) {
+      HPT_SOFT(cudaStreamSynchronize(server->engine->stream));
+      for (auto& kv : server->reqs)
+        if (kv.second->state == kRunning) server->engine->free_job(kv.second->buf);
+    }
+  }
+  delete server;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Autotuner
+// ===========================================================================
+namespace {
+
+std::string tune_key(const hpt_scene* scene, const hpt_render_params* p) {
+  cudaDeviceProp prop;
+  memset(&prop, 0, sizeof prop);
+  if (cudaGetDeviceProperties(&prop, scene->h.scene.device) != cudaSuccess) {
+    (void)cudaGetLastError();
+    snprintf(prop.name, sizeof prop.name, "unknown");
+  }
+  std::string dev(prop.name);
+  for (char& ch : dev)
+    if (ch == ' ' || ch == '|') ch = '_';
+  std::ostringstream k;
+  const hpt_scene_info& in = scene->h.scene.info;
+  k << dev << "|tris=" << in.num_triangles << "|nodes=" << in.num_device_nodes
+    << "|rays=" << (int64_t)p->sample_x * p->supersample_x * p->sample_y * p->supersample_y
+    << "|spp=" << p->sample << "|depth=" << p->depth;
+  return k.str();
+}
+
+bool cache_lookup(const char* path, const std::string& key, hpt_tuning* t) {
+  if (!path) return false;
+  std::ifstream f(path);
+  std::string line;
+  while (std::getline(f, line)) {
+    std::istringstream is(line);
+    std::string k;
+    hpt_tuning x = default_tuning();
+    if (!(is >> k >> x.capacity >> x.isect_block >> x.isect_min_blocks >> x.refill_chunk >>
+          x.smem_nodes >> x.use_graph))
+      continue;
+    if (k == key) {
+      *t = x;
+      return true;
+    }
+  }
+  return false;
+}
+
+void cache_store(const char* path, const std::string& key, const hpt_tuning& t) {
+  if (!path) return;
+  std::ofstream f(path, std::ios::app);
+  f << key << " " << t.capacity << " " << t.isect_block << " " << t.isect_min_blocks << " "
+    << t.refill_chunk << " " << t.smem_nodes << " " << t.use_graph << "\n";
+}
+
+}  // namespace
+
+extern "C" hpt_status hpt_autotune(hpt_scene* scene, const hpt_camera* camera,
+                                   const hpt_render_params* params, const char* cache_path,
+                                   hpt_tuning* best) {
+  if (!scene) return fail(HPT_ERR_INVALID_ARGUMENT, "scene is NULL");
+  hpt_status s = check_render_params(camera, params);
+  if (s != HPT_OK) return s;
+  const std::string key = tune_key(scene, params);
+  hpt_tuning cur;
+  {
+    std::lock_guard<std::mutex> lk(scene->h.mu);
+    cur = scene->h.tuning;
+  }
+  if (cache_lookup(cache_path, key, &cur)) {
+    std::lock_guard<std::mutex> lk(scene->h.mu);
+    cur.profile = scene->h.tuning.profile;
+    cur.shade_block = 256;
+    scene->h.tuning = cur;
+    scene->h.engine.reset();
+    if (best) *best = cur;
+    return HPT_OK;
+  }
+  // Device time of one render with tuning t (best of two after a warm-up).
+  auto time_of = [&](const hpt_tuning& t, float* ms) -> hpt_status {
+    std::lock_guard<std::mutex> lk(scene->h.mu);
+    Engine e(scene->h.scene.device);
+    e.tuning = t;
+    JobSpec js;
+    js.scene = &scene->h.scene;
+    js.camera = *camera;
+    js.params = *params;
+    float bestms = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+      hpt_render_stats st;
+      hpt_status r = e.run({js}, &st);
+      if (r != HPT_OK) return r;
+      if (rep > 0) bestms = std::min(bestms, st.ms_total);
+    }
+    *ms = bestms;
+    return HPT_OK;
+  };
+  float cur_ms = 0.f;
+  s = time_of(cur, &cur_ms);
+  if (s != HPT_OK) return s;
+  // Coordinate search: one knob at a time, keeping the best value.
+  struct Knob {
+    std::vector<std::pair<int, int>> values;  // (a, b); b used by the variant knob
+    void (*apply)(hpt_tuning&, int, int);
+  };
+  const Knob knobs[] = {
+      {{{128, 5}, {128, 6}, {128, 8}, {256, 2}, {256, 3}},
+       [](hpt_tuning& t, int a, int b) {
+         t.isect_block = a;
+         t.isect_min_blocks = b;
+       }},
+      {{{2, 0}, {4, 0}, {8, 0}, {16, 0}},
+       [](hpt_tuning& t, int a, int) { t.refill_chunk = a; }},
+      {{{0, 0}, {1024, 0}, {2048, 0}, {4096, 0}},
+       [](hpt_tuning& t, int a, int) { t.smem_nodes = a; }},
+      {{{1 << 20, 0}, {1 << 21, 0}, {1 << 22, 0}},
+       [](hpt_tuning& t, int a, int) { t.capacity = a; }},
+      {{{0, 0}, {1, 0}}, [](hpt_tuning& t, int a, int) { t.use_graph = a; }},
+  };
+  for (const Knob& k : knobs) {
+    for (const auto& v : k.values) {
+      hpt_tuning t = cur;
+      k.apply(t, v.first, v.second);
+      if (memcmp(&t, &cur, sizeof t) == 0) continue;
+      float ms = 0.f;
+      s = time_of(t, &ms);
+      if (s != HPT_OK) return s;
+      if (ms < cur_ms * 0.99f) {
+        cur = t;
+        cur_ms = ms;
+      }
+    }
+  }
+  cache_store(cache_path, key, cur);
+  {
+    std::lock_guard<std::mutex> lk(scene->h.mu);
+    cur.profile = scene->h.tuning.profile;
+    cur.shade_block = 256;
+    scene->h.tuning = cur;
+    scene->h.engine.reset();
+  }
+  if (best) *best = cur;
+  return HPT_OK;
 }

@@ -418,6 +418,10 @@ hpt_status hpt_server_poll(hpt_server* server, uint64_t request_id,
 hpt_status hpt_server_cancel(hpt_server* server, uint64_t request_id);
 /* Requests queued + running. */
 int32_t hpt_server_pending(const hpt_server* server);
+/* Cumulative device counters of the server's wavefront (intersect queries
+ * including primary rays, shade calls, iterations, traversal work); `paths`
+ * holds the number of completed requests. */
+hpt_status hpt_server_stats_get(hpt_server* server, hpt_render_stats* out);
 void hpt_server_destroy(hpt_server* server);
 
 /* ---------------------------------------------------------------------- */
