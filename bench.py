@@ -17,6 +17,7 @@ collective): weak scaling.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -43,6 +44,17 @@ def parse():
     # Overrides for profiling runs only (the headline workload is the default).
     ap.add_argument("--res", type=int, default=0)
     ap.add_argument("--spp", type=int, default=0)
+    # Extra workloads (one JSON line each): the 32-job mixed batch, batched
+    # vs one job at a time; the Poisson serving stream.
+    ap.add_argument("--mode", default="frame", choices=["frame", "batch", "serve"])
+    ap.add_argument("--rate", default="50", help="serve: requests per second (comma list)")
+    ap.add_argument("--duration", type=float, default=4.0, help="serve: seconds of arrivals")
+    ap.add_argument("--serve-capacity", type=int, default=1 << 20,
+                    help="serve: wavefront capacity (paths in flight)")
+    ap.add_argument("--large-pct", type=int, default=25,
+                    help="serve: in-flight cap of requests larger than the wavefront, %%")
+    ap.add_argument("--terrain-n", type=int, default=1024,
+                    help="serve: heightfield vertices per side of the large scenes")
     return ap.parse_args()
 
 
@@ -226,9 +238,248 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def rotate(v, axis, ang):
+    """Rodrigues rotation of v about the unit axis by ang radians."""
+    v = np.asarray(v, np.float64)
+    k = np.asarray(axis, np.float64)
+    k = k / np.linalg.norm(k)
+    return (v * math.cos(ang) + np.cross(k, v) * math.sin(ang) +
+            k * np.dot(k, v) * (1 - math.cos(ang)))
+
+
+def jitter_camera(cam, rng):
+    """A pose request: yaw and pitch within +-30 degrees, translation within
+    +-0.1 of the scene's base camera."""
+    top, right = np.asarray(cam["top_dir"]), np.asarray(cam["right_dir"])
+    yaw, pitch = np.radians(rng.uniform(-30, 30, 2))
+    right2 = rotate(right, top, yaw)
+    top2 = rotate(top, right2, pitch)
+    eye = np.asarray(cam["view_p"]) + rng.uniform(-0.1, 0.1, 3)
+    return dict(view_p=tuple(eye), top_dir=tuple(top2), right_dir=tuple(right2),
+                width=cam["width"], height=cam["height"])
+
+
+def c3_jobs(seed=0x48505403):
+    """The 32 mixed jobs: scene family 0-2, triangles log-uniform in
+    [1k, 500k], resolution in {128, 256, 512, 1024} squared, spp in
+    {1, 4, 16, 64}, depth uniform in [3, 10]."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for j in range(32):
+        jobs.append(dict(family=int(rng.integers(0, 3)),
+                         tris=int(round(math.exp(rng.uniform(math.log(1e3), math.log(5e5))))),
+                         res=int(rng.choice([128, 256, 512, 1024])),
+                         spp=int(rng.choice([1, 4, 16, 64])),
+                         depth=int(rng.integers(3, 11)), seed=7000 + j))
+    return jobs
+
+
+def run_batch(args):
+    """C3: 32 jobs one by one through hpt_render (the plain per-job path)
+    against the same jobs in one hpt_batch wavefront with the autotuned
+    tuning. Accumulators are compared bit for bit (counter RNG + fixed-point
+    sums), so the relMSE of both against the reference estimate is identical
+    by construction."""
+    import torch
+    import hptracing_b200 as H
+    from hptracing_b200 import build as hbuild
+    from tests import scenes as S
+    hbuild.build()
+    torch.cuda.set_device(0)
+    jobs = c3_jobs()
+    t0 = time.perf_counter()
+    built = []
+    for j in jobs:
+        mesh = H.Mesh.generate(3, seed=j["seed"], family=j["family"], target_triangles=j["tris"])
+        nodes, leaf = H.build_kdtree(mesh.points, mesh.triangles)
+        cam = S.terrain_cam(1.0) if j["family"] == 2 else S.ROOM_CAM
+        built.append((H.Scene(mesh, nodes, leaf), S.hp_camera(cam),
+                      H.make_params(j["res"], j["res"], 1, 1, (0.05, 0.05, 0.05), j["spp"],
+                                    j["depth"], 0, 1.0, j["seed"]), len(mesh.triangles)))
+    build_s = time.perf_counter() - t0
+    # Autotune on the job with the most rays x spp, at reduced spp.
+    big = max(range(len(jobs)), key=lambda k: jobs[k]["res"] ** 2 * jobs[k]["spp"])
+    sc, cam, p, _ = built[big]
+    probe = H.make_params(p.sample_x, p.sample_y, 1, 1, (0, 0, 0), min(4, p.sample), p.depth, 0,
+                          1.0, 1)
+    tune = sc.autotune(cam, probe)
+    for sc, _, _, _ in built:
+        sc.set_tuning(tune)
+
+    def plain():
+        q = ms = 0.0
+        accs = []
+        t = time.perf_counter()
+        for sc, cam, p, _ in built:
+            _, acc = sc.render(cam, p, want_accum=True)
+            st = sc.stats()
+            q += st["intersect_queries"]
+            ms += st["ms_total"]
+            accs.append(acc)
+        return q, ms, time.perf_counter() - t, accs
+
+    def batched():
+        b = H.Batch()
+        b.set_tuning(tune)
+        for sc, cam, p, _ in built:
+            b.add(sc, cam, p, want_accum=True)
+        t = time.perf_counter()
+        out = b.run()
+        wall = time.perf_counter() - t
+        st = b.stats()
+        b.close()
+        return st["intersect_queries"], st["ms_total"], wall, [o[1] for o in out]
+
+    plain()
+    batched()
+    q_p, ms_p, wall_p, acc_p = plain()
+    q_b, ms_b, wall_b, acc_b = batched()
+    same = all(np.array_equal(a, b) for a, b in zip(acc_p, acc_b))
+    work = [j["res"] ** 2 * j["spp"] * j["depth"] for j in jobs]
+    line = {
+        "metric": "Mrays/s batched vs plain (C3, 32 mixed jobs)", "mode": "batch",
+        "value": q_b / ms_b / 1e3, "unit": "Mrays/s", "plain": q_p / ms_p / 1e3,
+        "speedup": (q_b / ms_b) / (q_p / ms_p), "higher_is_better": True, "n_gpus": 1,
+        "ms_batched": ms_b, "ms_plain": ms_p, "queries": q_b,
+        "e2e": {"batched": q_b / wall_b / 1e6, "plain": q_p / wall_p / 1e6, "unit": "Mrays/s"},
+        "accumulators_bit_identical": same,
+        "largest_job_share_of_work": max(work) / sum(work),
+        "tuning": {"capacity": tune.capacity, "isect_block": tune.isect_block,
+                   "isect_min_blocks": tune.isect_min_blocks, "refill": tune.refill_chunk,
+                   "smem_nodes": tune.smem_nodes, "use_graph": tune.use_graph},
+        "jobs": [dict(j, triangles=b[3]) for j, b in zip(jobs, built)],
+        "scene_build_s": build_s, "dtype": "f32", "data": "synthetic (seeded scene families)"}
+    print(json.dumps(line), flush=True)
+    for sc, _, _, _ in built:
+        sc.close()
+
+
+def run_serve(args):
+    """C4: Poisson arrivals over four resident scenes (box room, spheres,
+    terrain, a larger terrain). 80 % pose requests (512x512, 4 spp), 20 %
+    panoramas (2048x1024, 64 spp), depth 6. Latency = completion -
+    submission on the server's clock. The scenes are built once and every
+    rate of --rate runs against a fresh server."""
+    import torch
+    import hptracing_b200 as H
+    from hptracing_b200 import build as hbuild
+    from tests import scenes as S
+    hbuild.build()
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    specs = [(0, {}), (1, dict(seed=1)),
+             (2, dict(seed=2, heightfield_n=args.terrain_n)),
+             (2, dict(seed=3, heightfield_n=int(args.terrain_n * 1.33)))]
+    scenes, cams, tris = [], [], []
+    for cfg, kw in specs:
+        mesh = H.Mesh.generate(cfg, **kw)
+        nodes, leaf = H.build_kdtree(mesh.points, mesh.triangles)
+        scenes.append(H.Scene(mesh, nodes, leaf))
+        cams.append(S.terrain_cam(1.0) if cfg == 2 else S.ROOM_CAM)
+        tris.append(len(mesh.triangles))
+        del mesh, nodes, leaf
+    build_s = time.perf_counter() - t0
+    for rate in [float(x) for x in str(args.rate).split(",")]:
+        serve_stream(H, S, scenes, cams, tris, build_s, rate, args)
+    for sc in scenes:
+        sc.close()
+
+
+def serve_stream(H, S, scenes, cams, tris, build_s, rate, args):
+    """One Poisson stream at `rate` requests/s against a fresh server."""
+    server = H.Server(max_jobs=64, memory_budget=16 << 30, capacity=args.serve_capacity,
+                      large_inflight_pct=args.large_pct)
+    slots = [server.add_scene(s) for s in scenes]
+    rng = np.random.default_rng(0x48505404 + int(rate))
+    arrivals, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > args.duration:
+            break
+        k = int(rng.integers(0, 4))
+        if rng.random() < 0.8:
+            cam = jitter_camera(cams[k], rng)
+            p = H.make_params(512, 512, 1, 1, (0.05, 0.05, 0.05), 4, 6, 0, 1.0,
+                              int(rng.integers(1, 2 ** 31)))
+            arrivals.append((t, "pose", k, cam, p))
+        else:
+            pano = dict(view_p=cams[k]["view_p"], top_dir=(0.0, 1.0, 0.0),
+                        right_dir=(0.0, 0.0, 1.0), width=1.0, height=-1.0)
+            p = H.make_params(2048, 1024, 1, 1, (0.2, 0.2, 0.2), 64, 6, 0, 1.0,
+                              int(rng.integers(1, 2 ** 31)))
+            arrivals.append((t, "pano", k, pano, p))
+    # Warm-up: one small request per scene.
+    for k in range(4):
+        rid = server.submit(slots[k], S.hp_camera(cams[k]),
+                            H.make_params(128, 128, 1, 1, (0, 0, 0), 1, 6, 0, 1.0, 1))
+        while server.poll(rid)[0] != 0:
+            server.pump(1)
+    server.completed()
+    st0 = server.stats()
+    sampler = ClockSampler(0)
+    sampler.start()
+    start = time.perf_counter()
+    outstanding = {}
+    lat = {"pose": [], "pano": []}
+    samples = 0
+    nxt = 0
+    drain_cap = args.duration + 20.0
+    while True:
+        now = time.perf_counter() - start
+        while nxt < len(arrivals) and arrivals[nxt][0] <= now:
+            _, kind, k, cam, p = arrivals[nxt]
+            rid = server.submit(slots[k], S.hp_camera(cam), p)
+            outstanding[rid] = (kind, p)
+            nxt += 1
+        if not outstanding and nxt >= len(arrivals):
+            break
+        if now > drain_cap:
+            break
+        if outstanding:
+            server.pump(1)
+            for rid in server.completed():
+                st, info = server.poll(rid)
+                if st == 0 and rid in outstanding:
+                    kind, p = outstanding.pop(rid)
+                    lat[kind].append(info["done_ms"] - info["submit_ms"])
+                    samples += p.sample_x * p.sample_y * p.sample
+        else:
+            time.sleep(0.0005)
+    elapsed = time.perf_counter() - start
+    clocks = sampler.stop()
+    st1 = server.stats()
+    q = st1["intersect_queries"] - st0["intersect_queries"]
+
+    def pct(v, x):
+        return float(np.percentile(v, x)) if v else None
+
+    line = {
+        "metric": "serving p50/p99 latency (C4)", "mode": "serve", "rate_per_s": rate,
+        "duration_s": args.duration, "elapsed_s": elapsed,
+        "requests": len(arrivals), "completed": len(lat["pose"]) + len(lat["pano"]),
+        "unfinished": len(outstanding) + (len(arrivals) - nxt),
+        "pose_512x512_4spp": {"n": len(lat["pose"]), "p50_ms": pct(lat["pose"], 50),
+                              "p99_ms": pct(lat["pose"], 99)},
+        "pano_2048x1024_64spp": {"n": len(lat["pano"]), "p50_ms": pct(lat["pano"], 50),
+                                 "p99_ms": pct(lat["pano"], 99)},
+        "Mrays_per_s": q / elapsed / 1e6, "Msamples_per_s": samples / elapsed / 1e6,
+        "server": {"capacity": args.serve_capacity, "large_inflight_pct": args.large_pct,
+                   "max_jobs": 64, "memory_budget": 16 << 30},
+        "scene_triangles": tris, "scene_build_s": build_s, "clocks": clocks,
+        "dtype": "f32", "data": "synthetic (seeded scenes, seeded Poisson stream)"}
+    print(json.dumps(line), flush=True)
+    server.close()
+
+
 def main():
     global W_RES, H_RES, SPP, WORKLOAD
     args = parse()
+    if args.mode == "batch":
+        run_batch(args)
+        return
+    if args.mode == "serve":
+        run_serve(args)
+        return
     if args.res or args.spp:
         W_RES = H_RES = args.res or W_RES
         SPP = args.spp or SPP

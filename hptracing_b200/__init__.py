@@ -28,6 +28,15 @@ __all__ = ["Mesh", "KDTree", "Scene", "TraceRunner", "Batch", "Server", "build_k
            "MATERIAL_DTYPE"]
 
 
+
+def _copy_out(address, nbytes, dtype):
+    """Copies nbytes at a C address into a new numpy array (sizes above
+    2 GiB included, which ctypes.string_at cannot take)."""
+    if not isinstance(address, int):
+        address = C.cast(address, C.c_void_p).value
+    buf = (C.c_uint8 * nbytes).from_address(address)
+    return np.frombuffer(buf, dtype=np.uint8).view(dtype).copy()
+
 def device_count():
     return lib().hpt_device_count()
 
@@ -95,11 +104,10 @@ class Mesh:
         m.triangles = arr(v.triangles, v.num_triangles, 4, np.int32)
         m.lights = arr(v.lights, v.num_lights, 4, np.int32)
         nb = v.num_materials * MATERIAL_DTYPE.itemsize
-        m.materials = (np.frombuffer(C.string_at(v.materials, nb), dtype=MATERIAL_DTYPE).copy()
+        m.materials = (_copy_out(v.materials, nb, MATERIAL_DTYPE)
                        if nb else np.zeros(0, MATERIAL_DTYPE))
         m.texture_dims = arr(v.texture_dims, v.num_textures, 2, np.int32)
-        m.texture_data = (np.frombuffer(C.string_at(v.texture_data, v.texture_bytes),
-                                        dtype=np.uint8).copy()
+        m.texture_data = (_copy_out(v.texture_data, v.texture_bytes, np.uint8)
                           if v.texture_bytes else np.zeros(0, np.uint8))
         m.texture_names = ["tex%d" % i for i in range(v.num_textures)]
         lib().hpt_mesh_destroy(h)
@@ -144,8 +152,8 @@ def build_kdtree(points, triangles, threads=0):
         lp = C.c_void_p()
         nl = C.c_int32()
         check(lib().hpt_kdtree_view(h, C.byref(np_), C.byref(nn), C.byref(lp), C.byref(nl)))
-        nodes = np.frombuffer(C.string_at(np_, nn.value * 48), dtype=NODE_DTYPE).copy()
-        leaf = np.frombuffer(C.string_at(lp, nl.value * 4), dtype=np.int32).copy()
+        nodes = _copy_out(np_, nn.value * 48, NODE_DTYPE)
+        leaf = _copy_out(lp, nl.value * 4, np.int32)
     finally:
         lib().hpt_kdtree_destroy(h)
     return nodes, leaf
@@ -429,8 +437,9 @@ class Server:
     """Continuous-batching render server (hpt_server)."""
 
     def __init__(self, device=0, max_jobs=64, memory_budget=8 << 30, capacity=1 << 22,
-                 progressive=0):
-        cfg = ServerConfig(device, max_jobs, memory_budget, capacity, progressive)
+                 progressive=0, large_inflight_pct=0):
+        cfg = ServerConfig(device, max_jobs, memory_budget, capacity, progressive,
+                           large_inflight_pct)
         h = C.c_void_p()
         check(lib().hpt_server_create(C.byref(cfg), C.byref(h)))
         self._h = h
@@ -463,6 +472,13 @@ class Server:
 
     def pending(self):
         return lib().hpt_server_pending(self._h)
+
+    def completed(self, max_ids=4096):
+        """Ids of the requests that finished since the previous call."""
+        ids = np.zeros(max_ids, np.uint64)
+        n = C.c_int32()
+        check(lib().hpt_server_drain_completed(self._h, ptr(ids), max_ids, C.byref(n)))
+        return [int(x) for x in ids[:n.value]]
 
     def stats(self):
         s = RenderStats()

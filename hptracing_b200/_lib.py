@@ -98,7 +98,7 @@ class Tuning(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("device", i32), ("max_jobs", i32), ("memory_budget", i64), ("capacity", i32),
-                ("progressive", i32), ("reserved", i32 * 4)]
+                ("progressive", i32), ("large_inflight_pct", i32), ("reserved", i32 * 3)]
 
 
 class RequestInfo(C.Structure):
@@ -150,6 +150,7 @@ SIGNATURES = {
     "hpt_server_cancel": (i32, [vp, u64]),
     "hpt_server_pending": (i32, [vp]),
     "hpt_server_stats_get": (i32, [vp, P(RenderStats)]),
+    "hpt_server_drain_completed": (i32, [vp, vp, i32, P(i32)]),
     "hpt_server_destroy": (None, [vp]),
     "hpt_autotune": (i32, [vp, P(Camera), P(RenderParams), C.c_char_p, P(Tuning)]),
 }

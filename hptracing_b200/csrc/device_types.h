@@ -99,6 +99,7 @@ struct DevJob {
   uint32_t* flags;          // per ray: NaN / +inf / -inf markers (4 bits per channel)
   float* prim;              // primary hit cache, 8 floats per entry
   int32_t* prim_count;      // number of primary hits
+  int64_t max_inflight;     // cap on started-but-unfinished paths (0 = none)
 };
 
 // Scheduling state of a slot. A job's paths are (primary hit k, sample s)
@@ -108,6 +109,7 @@ struct DevSlot {
   int64_t cursor;
   unsigned long long done;  // paths finished (flushed)
   unsigned long long queries;  // secondary intersect queries issued
+  int64_t max_inflight;     // copied from the job at admission (0 = none)
   int32_t alloc;            // new paths granted for the coming shade pass
   int32_t active;           // admitted and not yet fully issued
 };

@@ -173,7 +173,12 @@ __device__ void schedule(const EngineParams& P) {
     const int64_t rem = S.num_paths - S.cursor;
     if (rem <= 0) continue;
     remaining = true;
-    const int a = (int)min(rem, (int64_t)(budget - n_new));
+    int64_t grant = min(rem, (int64_t)(budget - n_new));
+    // A capped job (e.g. a large request that must not crowd out the
+    // latency-sensitive ones behind it) keeps at most max_inflight paths
+    // started and unfinished.
+    if (S.max_inflight > 0) grant = min(grant, S.max_inflight - (S.cursor - (int64_t)S.done));
+    const int a = (int)grant;
     if (a <= 0) continue;
     S.alloc = a;
     P.quota_slot[nq] = s;
@@ -272,6 +277,7 @@ __global__ void k_admit(EngineParams P) {
     S.cursor = 0;
     S.done = 0;
     S.queries = 0;
+    S.max_inflight = P.jobs[s].max_inflight;
     S.alloc = 0;
     S.active = 1;
   }
@@ -1086,6 +1092,18 @@ hpt_status Engine::read_slots(std::vector<DevSlot>& out) {
                            cudaMemcpyDeviceToHost, stream));
   HPT_CUDA(cudaStreamSynchronize(stream));
   std::copy(slots_host_, slots_host_ + slots_, out.begin());
+  return HPT_OK;
+}
+
+hpt_status Engine::read_state(std::vector<DevSlot>& slots, DevCtrl* ctrl) {
+  slots.resize(slots_);
+  if (slots_ > 0)
+    HPT_CUDA(cudaMemcpyAsync(slots_host_, slot_state_, (size_t)slots_ * sizeof(DevSlot),
+                             cudaMemcpyDeviceToHost, stream));
+  HPT_CUDA(cudaMemcpyAsync(ctrl_host_, ctrl_, sizeof(DevCtrl), cudaMemcpyDeviceToHost, stream));
+  HPT_CUDA(cudaStreamSynchronize(stream));
+  std::copy(slots_host_, slots_host_ + slots_, slots.begin());
+  *ctrl = *ctrl_host_;
   return HPT_OK;
 }
 

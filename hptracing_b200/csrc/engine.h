@@ -86,6 +86,7 @@ class Engine {
   // Synchronous read-back of the slot table / control block.
   hpt_status read_slots(std::vector<DevSlot>& out);
   hpt_status read_ctrl(DevCtrl* out);
+  hpt_status read_state(std::vector<DevSlot>& slots, DevCtrl* ctrl);  // one sync
   void reset_ctrl();
   DevCtrl* ctrl_dev() const { return ctrl_; }
   DevSlot* slots_dev() const { return slot_state_; }

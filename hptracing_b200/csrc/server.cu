@@ -65,6 +65,8 @@ struct hpt_server {
   uint64_t next_id = 1;
   std::chrono::steady_clock::time_point t0;
   std::vector<DevSlot> slot_view;
+  DevCtrl ctrl_view{};
+  std::vector<uint64_t> finished_ids;  // since the last hpt_server_drain_completed
   int64_t completed = 0;
   int64_t pumps = 0;
 
@@ -103,7 +105,10 @@ hpt_status hpt_server::admit_pending() {
   for (auto it = queue.begin(); it != queue.end();) {
     Request* r = find(*it);
     if (!r || r->cancel) {
-      if (r) r->state = kCancelled;
+      if (r) {
+        r->state = kCancelled;
+        finished_ids.push_back(r->id);
+      }
       it = queue.erase(it);
       continue;
     }
@@ -130,7 +135,11 @@ hpt_status hpt_server::admit_pending() {
     slot_req[slot] = r->id;
     used_bytes += r->footprint;
     ids.push_back(slot);
-    jobs.push_back(engine->make_job(r->js, r->buf));
+    DevJob dj = engine->make_job(r->js, r->buf);
+    const int pct = cfg.large_inflight_pct;
+    if (pct > 0 && pct < 100 && r->rays * r->js.params.sample > (int64_t)cfg.capacity)
+      dj.max_inflight = std::max<int64_t>(1024, (int64_t)cfg.capacity * pct / 100);
+    jobs.push_back(dj);
     rays.push_back(r->rays);
     it = queue.erase(it);
   }
@@ -141,7 +150,7 @@ hpt_status hpt_server::admit_pending() {
 // Reads the slot table; resolves, copies back and releases every request
 // whose paths have all finished.
 hpt_status hpt_server::collect() {
-  hpt_status s = engine->read_slots(slot_view);
+  hpt_status s = engine->read_state(slot_view, &ctrl_view);
   if (s != HPT_OK) return s;
   std::vector<Request*> finished;
   for (size_t k = 0; k < slot_req.size(); ++k) {
@@ -175,6 +184,7 @@ hpt_status hpt_server::collect() {
     r->slot = -1;
     r->state = r->cancel ? kCancelled : kDone;
     r->done_ms = t;
+    finished_ids.push_back(r->id);
     ++completed;
   }
   return engine->set_order(order());
@@ -186,7 +196,8 @@ hpt_status hpt_server_create(const hpt_server_config* config, hpt_server** out) 
   if (!config || !out) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
   *out = nullptr;
   if (config->max_jobs < 1 || config->max_jobs > 4096 || config->memory_budget <= 0 ||
-      config->capacity < 1024 || config->capacity > (1 << 27))
+      config->capacity < 1024 || config->capacity > (1 << 27) ||
+      config->large_inflight_pct < 0 || config->large_inflight_pct > 100)
     return fail(HPT_ERR_INVALID_ARGUMENT, "server config out of range");
   if (config->device < 0 || config->device >= hpt_device_count())
     return fail(HPT_ERR_CUDA, "no CUDA device %d", config->device);
@@ -261,9 +272,7 @@ hpt_status hpt_server_pump(hpt_server* server, int32_t max_iterations) {
   ++server->pumps;
   s = server->collect();
   if (s != HPT_OK) return s;
-  DevCtrl c;
-  s = server->engine->read_ctrl(&c);
-  if (s != HPT_OK) return s;
+  const DevCtrl& c = server->ctrl_view;
   if (c.err.flags & 2u)
     return fail(HPT_ERR_INVALID_SCENE, "device self-check %d failed (value %lld)", c.err.site,
                 (long long)c.err.value);
@@ -322,6 +331,18 @@ hpt_status hpt_server_cancel(hpt_server* server, uint64_t request_id) {
   if (!r) return fail(HPT_ERR_NOT_FOUND, "unknown request %llu", (unsigned long long)request_id);
   r->cancel = true;  // queued: dropped at the next admission; running: discarded when done
   if (r->state == kQueued) r->state = kCancelled;
+  return HPT_OK;
+}
+
+hpt_status hpt_server_drain_completed(hpt_server* server, uint64_t* ids, int32_t max_ids,
+                                      int32_t* count) {
+  if (!server || !count || max_ids < 0 || (max_ids > 0 && !ids))
+    return fail(HPT_ERR_INVALID_ARGUMENT, "bad drain arguments");
+  std::lock_guard<std::mutex> lk(server->mu);
+  const int32_t n = std::min<int32_t>(max_ids, (int32_t)server->finished_ids.size());
+  std::copy(server->finished_ids.begin(), server->finished_ids.begin() + n, ids);
+  server->finished_ids.erase(server->finished_ids.begin(), server->finished_ids.begin() + n);
+  *count = n;
   return HPT_OK;
 }
 

@@ -385,7 +385,11 @@ typedef struct hpt_server_config {
   int64_t memory_budget;      /* bytes of per-request device state        */
   int32_t capacity;           /* paths in flight shared by all requests   */
   int32_t progressive;        /* stream partial accumulations             */
-  int32_t reserved[4];
+  /* A request with more paths (rays x spp) than `capacity` keeps at most
+   * this percentage of `capacity` in flight, so it cannot crowd out the
+   * smaller requests admitted after it (0 or 100 = no cap). */
+  int32_t large_inflight_pct;
+  int32_t reserved[3];
 } hpt_server_config;
 
 typedef struct hpt_request_info {
@@ -416,6 +420,11 @@ hpt_status hpt_server_poll(hpt_server* server, uint64_t request_id,
                            hpt_request_info* info, uint8_t* rgba_out,
                            float* accum_out);
 hpt_status hpt_server_cancel(hpt_server* server, uint64_t request_id);
+/* Ids of requests that finished (done, cancelled or failed) since the
+ * previous call, oldest first; at most max_ids, *count of them. Lets a host
+ * poll only finished requests. */
+hpt_status hpt_server_drain_completed(hpt_server* server, uint64_t* ids,
+                                      int32_t max_ids, int32_t* count);
 /* Requests queued + running. */
 int32_t hpt_server_pending(const hpt_server* server);
 /* Cumulative device counters of the server's wavefront (intersect queries

@@ -65,8 +65,12 @@ def _drain(server, ids, reqs, max_pumps=20000):
     raise AssertionError("server did not finish: %d of %d" % (len(out), len(ids)))
 
 
-def test_results_alone_equal_results_in_the_mix(scenes):
-    server = H.Server(max_jobs=8, memory_budget=1 << 30, capacity=1 << 16)
+@pytest.mark.parametrize("capacity,large_pct", [(1 << 16, 0), (1 << 14, 25)])
+def test_results_alone_equal_results_in_the_mix(scenes, capacity, large_pct):
+    # With capacity 2^14 most requests exceed one wavefront and run capped at
+    # 25 % of it in flight: scheduling changes, results must not.
+    server = H.Server(max_jobs=8, memory_budget=1 << 30, capacity=capacity,
+                      large_inflight_pct=large_pct)
     slots = [server.add_scene(s) for s in scenes]
     # Staggered arrivals: half submitted up front, the rest while the first
     # half runs (continuous batching into freed slots).
@@ -105,6 +109,8 @@ def test_admission_respects_the_memory_budget(scenes):
     out = _drain(server, ids, reqs)
     for rid, r in zip(ids, reqs):
         assert np.array_equal(out[rid][1], _alone(scenes, r)[1])
+    assert sorted(server.completed()) == sorted(ids)
+    assert server.completed() == []
     # A request larger than the whole budget is refused at submission.
     big = H.make_params(1024, 1024, 1, 1, (0, 0, 0), 1, 5, 0, 1.0, 1)
     with pytest.raises(H.HptError) as e:
@@ -134,9 +140,8 @@ def test_progressive_previews_and_cancel(scenes):
     with pytest.raises(H.HptError) as e:
         server.poll(victim)
     assert e.value.status in (6, 8)
-    final = np.zeros((64, 64, 4), np.uint8)
-    _, a = _alone(scenes, req)
-    assert np.abs(previews[-1].astype(int) - _alone(scenes, req)[0].astype(int)).mean() < 40
+    final_rgba = _alone(scenes, req)[0]
+    assert np.abs(previews[-1].astype(int) - final_rgba.astype(int)).mean() < 40
     server.close()
 
 
