@@ -346,7 +346,8 @@ def run_batch(args):
         "largest_job_share_of_work": max(work) / sum(work),
         "tuning": {"capacity": tune.capacity, "isect_block": tune.isect_block,
                    "isect_min_blocks": tune.isect_min_blocks, "refill": tune.refill_chunk,
-                   "smem_nodes": tune.smem_nodes, "use_graph": tune.use_graph},
+                   "smem_nodes": tune.smem_nodes, "use_graph": tune.use_graph,
+                   "trav_steps": tune.trav_steps},
         "jobs": [dict(j, triangles=b[3]) for j, b in zip(jobs, built)],
         "scene_build_s": build_s, "dtype": "f32", "data": "synthetic (seeded scene families)"}
     print(json.dumps(line), flush=True)

@@ -404,12 +404,14 @@ void release_scene(SceneDev& s) {
 namespace {
 
 // Ranges the engine supports (capacity: queue entries; smem_nodes: shared
-// node prefix; isect_block / isect_min_blocks: a compiled traversal variant,
+// node prefix; trav_steps: 0 = leaf per round, 1..256 step units per round;
+// isect_block / isect_min_blocks: a compiled traversal variant,
 // 0 min blocks = the block size's default).
 hpt_status check_tuning(const hpt_tuning& t) {
   if (t.capacity < 1024 || t.capacity > (1 << 27) || t.smem_nodes < 0 ||
       t.smem_nodes > kMaxSmemNodes || t.refill_chunk < 1 || t.refill_chunk > 32 ||
-      (t.isect_block != 128 && t.isect_block != 256) || t.isect_min_blocks < 0)
+      (t.isect_block != 128 && t.isect_block != 256) || t.isect_min_blocks < 0 ||
+      t.trav_steps < 0 || t.trav_steps > 256)
     return fail(HPT_ERR_INVALID_ARGUMENT, "tuning out of range");
   return HPT_OK;
 }

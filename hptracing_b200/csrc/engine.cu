@@ -68,6 +68,7 @@ struct EngineParams {
   int capacity;
   int smem_nodes;       // > 0 only when every job uses shared_nodes' scene
   int refill;
+  int trav_steps;       // > 0: step-at-a-time traversal, units per round
   const DevNode* shared_nodes;
 };
 
@@ -433,7 +434,10 @@ __global__ void __launch_bounds__(BS) k_shade(EngineParams P) {
 // ---------------------------------------------------------------------------
 // Intersect queue -> next shade queue, persistent warps with lane refill.
 // ---------------------------------------------------------------------------
-template <int BS, int MINB>
+// kStep: traverse with trav_step, P.trav_steps units per lane between refill
+// checks (lanes move to their next leaf independently); else one leaf per
+// lane per round with trav_leaf.
+template <int BS, int MINB, bool kStep>
 __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
   extern __shared__ uint2 snodes[];
   const int n_smem = stage_nodes(P, snodes);
@@ -443,6 +447,7 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
   const int lane = threadIdx.x & 31;
   bool active = false;
   TravState st;
+  StepState ss;
   int item = 0;   // index in the intersect queue; the payload is reloaded at the end
   int slot = 0;
   unsigned long long queries = 0;
@@ -466,6 +471,7 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
             if (ok) {
               trav_init(P.jobs[slot].scene, Ray{mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z)}, st,
                         __float_as_int(P.R_r[i].w));
+              if (kStep) step_init(ss);
               active = true;
               ++queries;
             }
@@ -475,7 +481,18 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
     }
     if (__ballot_sync(kFull, active) == 0) break;
     bool finished = false;
-    if (active) finished = trav_leaf(P.jobs[slot].scene, st, snodes, n_smem, &c->err, cnt);
+    if (active) {
+      if constexpr (kStep) {
+        const DevScene& sc = P.jobs[slot].scene;
+        for (int u = 0; u < P.trav_steps; ++u)
+          if (trav_step(sc, st, ss, snodes, n_smem, &c->err, cnt)) {
+            finished = true;
+            break;
+          }
+      } else {
+        finished = trav_leaf(P.jobs[slot].scene, st, snodes, n_smem, &c->err, cnt);
+      }
+    }
     const bool hit = finished && st.best.rec >= 0;
     const unsigned hm = __ballot_sync(kFull, hit);
     if (hm) {
@@ -549,15 +566,17 @@ __global__ void k_ctrl(EngineParams P) {
 // tighter budgets trade spills for resident warps. Chosen by the tuning.
 struct IsectVariant {
   int block, min_blocks;
-  void (*isect)(EngineParams);
+  void (*isect)(EngineParams);       // one leaf per round
+  void (*isect_step)(EngineParams);  // step-at-a-time
   void (*primary)(EngineParams);
 };
 const IsectVariant kIsectVariants[] = {
-    {128, 5, k_isect<128, 5>, k_primary<128, 5>},
-    {128, 6, k_isect<128, 6>, k_primary<128, 6>},
-    {128, 8, k_isect<128, 8>, k_primary<128, 8>},
-    {256, 2, k_isect<256, 2>, k_primary<256, 2>},
-    {256, 3, k_isect<256, 3>, k_primary<256, 3>},
+    {128, 5, k_isect<128, 5, false>, k_isect<128, 5, true>, k_primary<128, 5>},
+    {128, 6, k_isect<128, 6, false>, k_isect<128, 6, true>, k_primary<128, 6>},
+    {128, 7, k_isect<128, 7, false>, k_isect<128, 7, true>, k_primary<128, 7>},
+    {128, 8, k_isect<128, 8, false>, k_isect<128, 8, true>, k_primary<128, 8>},
+    {256, 2, k_isect<256, 2, false>, k_isect<256, 2, true>, k_primary<256, 2>},
+    {256, 3, k_isect<256, 3, false>, k_isect<256, 3, true>, k_primary<256, 3>},
 };
 constexpr int kNumIsectVariants = sizeof(kIsectVariants) / sizeof(kIsectVariants[0]);
 
@@ -641,13 +660,17 @@ void cuda_soft_fail(cudaError_t e, const char* what) {
 hpt_tuning default_tuning() {
   hpt_tuning t;
   memset(&t, 0, sizeof t);
+  // From the tuning sweep on the 61k-triangle spheres frame (512x512, 64 spp):
+  // step-at-a-time traversal, 24 units per refill check, 7 blocks of 128 per
+  // SM, no shared-node prefix.
   t.capacity = 1 << 22;
   t.isect_block = 128;
-  t.isect_min_blocks = 5;
+  t.isect_min_blocks = 7;
   t.shade_block = 256;
   t.refill_chunk = 4;
-  t.smem_nodes = 2048;
+  t.smem_nodes = 0;
   t.use_graph = 0;
+  t.trav_steps = 24;
   return t;
 }
 
@@ -845,6 +868,8 @@ static hpt_status raise_smem_limits(int device) {
   for (const IsectVariant& v : kIsectVariants) {
     HPT_CUDA(cudaFuncSetAttribute(v.primary, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     HPT_CUDA(cudaFuncSetAttribute(v.isect, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    HPT_CUDA(cudaFuncSetAttribute(v.isect_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  bytes));
   }
   done[device] = 1;
   return HPT_OK;
@@ -857,7 +882,8 @@ hpt_status Engine::query_occupancy() {
   const IsectVariant& v = kIsectVariants[isect_variant()];
   const size_t smem = (size_t)std::max(0, tuning.smem_nodes) * sizeof(uint2);
   int b = 0;
-  HPT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, v.isect, v.block, smem));
+  HPT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &b, tuning.trav_steps > 0 ? v.isect_step : v.isect, v.block, smem));
   occ_isect_ = std::max(1, b);
   HPT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<256>, 256, 0));
   occ_shade_ = std::max(1, b);
@@ -957,6 +983,7 @@ static EngineParams make_params(const Engine& e, DevCtrl* ctrl, DevJob* jobs, De
   P.R_r = R[3];
   P.capacity = capacity;
   P.refill = std::max(1, std::min(32, e.tuning.refill_chunk));
+  P.trav_steps = std::max(0, e.tuning.trav_steps);
   if (shared && e.tuning.smem_nodes > 0) {
     P.smem_nodes = std::min(e.tuning.smem_nodes, shared->num_nodes);
     P.shared_nodes = shared->nodes;
@@ -1032,7 +1059,8 @@ hpt_status Engine::ensure_graph(const DevScene* shared_scene, int iterations) {
   const void* key_nodes = shared_scene ? (const void*)shared_scene->nodes : nullptr;
   if (graph_exec_ && graph_nodes_ == key_nodes && graph_capacity_ == capacity_ &&
       graph_slots_ == slots_ && graph_iters_ == iterations && graph_tuning_ == isect_variant() &&
-      graph_smem_ == tuning.smem_nodes && graph_refill_ == tuning.refill_chunk)
+      graph_smem_ == tuning.smem_nodes && graph_refill_ == tuning.refill_chunk &&
+      graph_steps_ == tuning.trav_steps)
     return HPT_OK;
   if (graph_exec_) {
     HPT_SOFT(cudaGraphExecDestroy(graph_exec_));
@@ -1058,6 +1086,7 @@ hpt_status Engine::ensure_graph(const DevScene* shared_scene, int iterations) {
   graph_tuning_ = isect_variant();
   graph_smem_ = tuning.smem_nodes;
   graph_refill_ = tuning.refill_chunk;
+  graph_steps_ = tuning.trav_steps;
   return HPT_OK;
 }
 
@@ -1072,7 +1101,10 @@ void Engine::launch_iteration(const DevScene* shared_scene, cudaEvent_t* ev) {
   if (ev) HPT_SOFT(cudaEventRecord(ev[1], stream));
   const size_t smem = (size_t)P.smem_nodes * sizeof(uint2);
   const IsectVariant& v = kIsectVariants[isect_variant()];
-  v.isect<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
+  if (P.trav_steps > 0)
+    v.isect_step<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
+  else
+    v.isect<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
   if (ev) HPT_SOFT(cudaEventRecord(ev[2], stream));
   k_ctrl<<<1, 1, 0, stream>>>(P);
 }

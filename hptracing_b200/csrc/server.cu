@@ -421,7 +421,7 @@ bool cache_lookup(const char* path, const std::string& key, hpt_tuning* t) {
     std::string k;
     hpt_tuning x = default_tuning();
     if (!(is >> k >> x.capacity >> x.isect_block >> x.isect_min_blocks >> x.refill_chunk >>
-          x.smem_nodes >> x.use_graph))
+          x.smem_nodes >> x.use_graph >> x.trav_steps))
       continue;
     if (k == key) {
       *t = x;
@@ -435,7 +435,8 @@ void cache_store(const char* path, const std::string& key, const hpt_tuning& t) 
   if (!path) return;
   std::ofstream f(path, std::ios::app);
   f << key << " " << t.capacity << " " << t.isect_block << " " << t.isect_min_blocks << " "
-    << t.refill_chunk << " " << t.smem_nodes << " " << t.use_graph << "\n";
+    << t.refill_chunk << " " << t.smem_nodes << " " << t.use_graph << " " << t.trav_steps
+    << "\n";
 }
 
 }  // namespace
@@ -489,11 +490,13 @@ extern "C" hpt_status hpt_autotune(hpt_scene* scene, const hpt_camera* camera,
     void (*apply)(hpt_tuning&, int, int);
   };
   const Knob knobs[] = {
-      {{{128, 5}, {128, 6}, {128, 8}, {256, 2}, {256, 3}},
+      {{{128, 5}, {128, 6}, {128, 7}, {128, 8}, {256, 2}, {256, 3}},
        [](hpt_tuning& t, int a, int b) {
          t.isect_block = a;
          t.isect_min_blocks = b;
        }},
+      {{{0, 0}, {8, 0}, {16, 0}, {32, 0}},
+       [](hpt_tuning& t, int a, int) { t.trav_steps = a; }},
       {{{2, 0}, {4, 0}, {8, 0}, {16, 0}},
        [](hpt_tuning& t, int a, int) { t.refill_chunk = a; }},
       {{{0, 0}, {1024, 0}, {2048, 0}, {4096, 0}},

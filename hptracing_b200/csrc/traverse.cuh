@@ -294,4 +294,180 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, const uint2* smem,
   return false;
 }
 
+// --- Step-at-a-time traversal ----------------------------------------------
+// The same walk as trav_leaf, cut into units of similar cost: one descent
+// step, the set-up of a newly reached leaf, one triangle test, or the exit
+// of a finished leaf through its rope. A warp that calls trav_step in a loop
+// lets every lane move on to its next leaf as soon as its own leaf is done,
+// instead of waiting for the lane with the deepest descent and then for the
+// one with the longest triangle list; results are identical to trav_leaf's
+// (same tests in the same order, same termination).
+struct StepState {
+  int32_t phase;      // kStepDescend / kStepTest
+  int32_t k, end;     // next position in leaf_refs / end of the leaf's list
+  int32_t leaf;       // leaf record of the current leaf
+  int32_t leaf_node;  // its node index (reported as best_node)
+  int32_t face;       // exit face, -1 when the leaf has none
+  int32_t pierced;    // reference box test of the leaf: -1 not evaluated yet
+  float t_exit;
+};
+constexpr int32_t kStepDescend = 0;
+constexpr int32_t kStepTest = 1;
+
+HPT_HD void step_init(StepState& ss) {
+  ss.phase = kStepDescend;
+  ss.k = ss.end = 0;
+  ss.leaf = ss.leaf_node = 0;
+  ss.face = -1;
+  ss.pierced = -1;
+  ss.t_exit = 0.f;
+}
+
+// Returns true when the ray is finished.
+template <bool kUV = false>
+HPT_HD bool trav_step(const DevScene& s, TravState& st, StepState& ss, const uint2* smem,
+                      int n_smem, DevErr* err, TravCount& cnt) {
+  if (st.node < 0) return true;
+  const Ray& r = st.ray;
+  if (ss.phase == kStepDescend) {
+    HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
+    const uint2 nd = fetch_node(s, smem, n_smem, st.node);
+    if ((nd.x >> 30) != kLeafKind) {
+      // One descent step; the entry point p = o + t_entry * d on the split
+      // axis (kernel.cl:291 style, no FMA), as trav_leaf computes it.
+      const uint32_t axis = nd.x >> 30;
+      const float split = as_float_u(nd.y);
+      const float o = axis == 0 ? r.o.x : (axis == 1 ? r.o.y : r.o.z);
+      const float dd = axis == 0 ? r.d.x : (axis == 1 ? r.d.y : r.d.z);
+      const float p = rn_add(o, rn_mul(st.t_entry, dd));
+      const bool right = p > split || (p == split && dd > 0.f);
+      HPT_DCHECK(err, (int)(nd.x & kIndexMask) + 1 < s.num_nodes, 106, nd.x & kIndexMask,
+                 { st.node = -1; return true; });
+      st.node = (int)(nd.x & kIndexMask) + (right ? 1 : 0);
+      ++cnt.nodes;
+      if (++st.steps > s.max_steps) {
+        hpt_atomic_or(&err->flags, 1u);
+        st.node = -1;
+        return true;
+      }
+      return false;
+    }
+    // Leaf set-up: exit distance and face, triangle range.
+    HPT_DCHECK(err, (int)(nd.x & kIndexMask) < s.num_leaves, 102, nd.x & kIndexMask,
+               { st.node = -1; return true; });
+    const int leaf = (int)(nd.x & kIndexMask);
+    const float4* L = reinterpret_cast<const float4*>(s.leaves + leaf);
+    const float4 L0 = ldg(L), L1 = ldg(L + 1);
+    float t_exit = as_float(0x7f800000);
+    int face = -1;
+    {
+      const float d[3] = {r.d.x, r.d.y, r.d.z};
+      const float o[3] = {r.o.x, r.o.y, r.o.z};
+      const float iv[3] = {st.inv_d.x, st.inv_d.y, st.inv_d.z};
+      const float lo[3] = {L0.x, L0.y, L0.z};
+      const float hi[3] = {L1.x, L1.y, L1.z};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        if (d[a] != 0.f) {
+          const float tf = rn_mul(rn_sub(d[a] > 0.f ? hi[a] : lo[a], o[a]), iv[a]);
+          if (tf < t_exit) {
+            t_exit = tf;
+            face = 2 * a + (d[a] > 0.f ? 1 : 0);
+          }
+        }
+      }
+    }
+    const int begin = as_int(L0.w), count = as_int(L1.w);
+    ++cnt.leaves;
+    HPT_DCHECK(err, begin >= 0 && count >= 0 && (long long)begin + count <= s.num_leaf_tris, 103,
+               begin, { st.node = -1; return true; });
+    // trav_leaf adds the leaf's cost when it leaves it; every comparison with
+    // max_steps comes later in both orders, so adding it here is equivalent.
+    st.steps += 1 + count;
+    ss.k = begin;
+    ss.end = begin + count;
+    ss.leaf = leaf;
+    ss.leaf_node = st.node;
+    ss.face = face;
+    ss.t_exit = t_exit;
+    ss.pierced = -1;
+    ss.phase = kStepTest;
+    return false;
+  }
+  if (ss.k < ss.end) {
+    // One triangle test (the body of trav_leaf's triangle loop).
+    const int j = ss.k++;
+    const int id = ldg(s.leaf_refs + j);
+    HPT_DCHECK(err, id >= 0 && id < s.num_triangles, 104, id, return false);
+    const float4* recs = reinterpret_cast<const float4*>(s.tris);
+    float t = -1.f, u = 0.f, v = 0.f;
+    bool tested = false;
+    int slot = -1;
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+      if (st.mb_id[m] == id) slot = m;
+    if (slot >= 0) {
+      ++cnt.repeats;
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+        if (m == slot) t = st.mb_t[m];
+    } else {
+      ++cnt.tris;
+      const float4* rec = recs + 3 * (size_t)id;
+      const float4 A = ldg(rec), E1 = ldg(rec + 1), E2 = ldg(rec + 2);
+      if (!mt_test(r, A, E1, E2, t, u, v)) t = -1.f;
+      tested = true;
+      st.mb_id[3] = st.mb_id[2]; st.mb_t[3] = st.mb_t[2];
+      st.mb_id[2] = st.mb_id[1]; st.mb_t[2] = st.mb_t[1];
+      st.mb_id[1] = st.mb_id[0]; st.mb_t[1] = st.mb_t[0];
+      st.mb_id[0] = id; st.mb_t[0] = t;
+    }
+    if (t > 0.f && (st.best.rec < 0 || t < st.best.t || (t == st.best.t && j < st.best.rec))) {
+      if (ss.pierced < 0) {
+        const float4* L = reinterpret_cast<const float4*>(s.leaves + ss.leaf);
+        ss.pierced = ref_box_test(r, ldg(L), ldg(L + 1)) ? 1 : 0;
+      }
+      if (ss.pierced) {
+        if (kUV && !tested) {  // a repeat that now wins: recover its u, v
+          const float4* rec = recs + 3 * (size_t)id;
+          float t2;
+          mt_test(r, ldg(rec), ldg(rec + 1), ldg(rec + 2), t2, u, v);
+        }
+        st.best.rec = j;
+        st.best.tri = id;
+        st.best.t = t;
+        if (kUV) {
+          st.best.u = u;
+          st.best.v = v;
+        }
+        st.best_node = ss.leaf_node;
+      }
+    }
+    return false;
+  }
+  // Leaf exit: stop once the rest of the ray starts beyond the best hit
+  // (+ slack), else follow the exit rope.
+  ss.phase = kStepDescend;
+  if (ss.face < 0 || !(ss.t_exit < st.t_end)) {
+    st.node = -1;
+    return true;
+  }
+  if (st.best.rec >= 0 &&
+      ss.t_exit > rn_add(st.best.t, rn_add(rn_mul(st.best.t, 1e-4f), st.slack))) {
+    st.node = -1;
+    return true;
+  }
+  const int rope =
+      ldg(reinterpret_cast<const int*>(s.leaves + ss.leaf) + 8 + ss.face);
+  if (rope < 0 || st.steps > s.max_steps) {
+    if (rope >= 0) hpt_atomic_or(&err->flags, 1u);
+    st.node = -1;
+    return true;
+  }
+  HPT_DCHECK(err, rope < s.num_nodes, 105, rope, { st.node = -1; return true; });
+  st.node = rope;
+  st.t_entry = fmaxf(st.t_entry, ss.t_exit);
+  return false;
+}
+
 }  // namespace hpt

@@ -272,6 +272,10 @@ typedef struct hpt_tuning {
   int32_t use_graph;         /* capture the bounce loop in a CUDA graph   */
   int32_t profile;           /* time each stage with CUDA events          */
   int32_t isect_min_blocks;  /* register budget: blocks per SM to fit     */
+  int32_t trav_steps;        /* 0: one leaf per lane per round; n > 0:    */
+                             /* n traversal steps (descent step, leaf     */
+                             /* set-up, triangle test or leaf exit) per   */
+                             /* lane between refills                      */
 } hpt_tuning;
 hpt_status hpt_tuning_get(const hpt_scene* scene, hpt_tuning* out);
 hpt_status hpt_tuning_set(hpt_scene* scene, const hpt_tuning* in);

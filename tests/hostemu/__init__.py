@@ -23,6 +23,7 @@ def lib():
         L.emu_scene_destroy.argtypes = [vp]
         L.emu_scene_counts.argtypes = [vp, vp]
         L.emu_intersect.argtypes = [vp, C.c_int, vp, vp, vp, C.c_int, vp, vp, vp, vp, vp, vp, vp]
+        L.emu_intersect_step.argtypes = L.emu_intersect.argtypes
         L.emu_shade.argtypes = [vp, C.c_int] + [vp] * 6 + [C.c_int] + [vp] * 6
         L.emu_next_dir.argtypes = [vp, C.c_int] + [vp] * 11
         L.emu_tree.argtypes = [vp, vp, vp, vp]
@@ -65,7 +66,7 @@ class EmuScene:
         lib().emu_scene_counts(self.h, _p(c))
         return dict(nodes=int(c[0]), leaves=int(c[1]), refs=int(c[2]), max_depth=int(c[3]))
 
-    def intersect(self, o, d, hints=None, smem_nodes=0):
+    def intersect(self, o, d, hints=None, smem_nodes=0, step=False):
         o = np.ascontiguousarray(o, np.float32)
         d = np.ascontiguousarray(d, np.float32)
         n = len(o)
@@ -75,8 +76,9 @@ class EmuScene:
         cnt = np.zeros(4, np.int64)
         err = np.zeros(3, np.int64)
         h = None if hints is None else np.ascontiguousarray(hints, np.int32)
-        lib().emu_intersect(self.h, n, _p(o), _p(d), _p(h), smem_nodes, _p(tri), _p(t), _p(u),
-                            _p(v), _p(node), _p(cnt), _p(err))
+        fn = lib().emu_intersect_step if step else lib().emu_intersect
+        fn(self.h, n, _p(o), _p(d), _p(h), smem_nodes, _p(tri), _p(t), _p(u), _p(v), _p(node),
+           _p(cnt), _p(err))
         return dict(tri=tri, t=t, u=u, v=v, node=node, counts=cnt, err=err)
 
     def shade(self, o, d, strength, tri, t, seeds, disable_diffuse=0):

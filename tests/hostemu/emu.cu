@@ -133,6 +133,43 @@ void emu_intersect(void* h, int n, const float* o, const float* d, const int* hi
   err[2] = de.value;
 }
 
+// emu_intersect with the step-at-a-time traversal (trav_step).
+void emu_intersect_step(void* h, int n, const float* o, const float* d, const int* hints,
+                        int smem_nodes, int32_t* tri, float* t, float* u, float* v,
+                        int* best_node, long long* counters, long long* err) {
+  EmuScene* e = static_cast<EmuScene*>(h);
+  const DevScene& s = e->dev;
+  std::vector<uint2> smem((size_t)std::max(0, std::min(smem_nodes, s.num_nodes)));
+  for (size_t i = 0; i < smem.size(); ++i) {
+    smem[i].x = s.nodes[i].meta;
+    std::memcpy(&smem[i].y, &s.nodes[i].split, 4);
+  }
+  DevErr de;
+  memset(&de, 0, sizeof de);
+  TravCount cnt;
+  for (int i = 0; i < n; ++i) {
+    TravState st;
+    StepState ss;
+    step_init(ss);
+    trav_init(s, Ray{mk(o[3 * i], o[3 * i + 1], o[3 * i + 2]), mk(d[3 * i], d[3 * i + 1], d[3 * i + 2])},
+              st, hints ? hints[i] : -1);
+    while (!trav_step<true>(s, st, ss, smem.data(), (int)smem.size(), &de, cnt)) {
+    }
+    tri[i] = st.best.tri;
+    t[i] = st.best.rec >= 0 ? st.best.t : 0.f;
+    u[i] = st.best.rec >= 0 ? st.best.u : 0.f;
+    v[i] = st.best.rec >= 0 ? st.best.v : 0.f;
+    if (best_node) best_node[i] = st.best_node;
+  }
+  counters[0] = (long long)cnt.nodes;
+  counters[1] = (long long)cnt.leaves;
+  counters[2] = (long long)cnt.tris;
+  counters[3] = (long long)cnt.repeats;
+  err[0] = de.flags;
+  err[1] = de.site;
+  err[2] = de.value;
+}
+
 void emu_shade(void* h, int n, const float* o, const float* d, const float* strength,
                const int32_t* tri, const float* t, uint64_t* seeds, int disable_diffuse,
                float* contrib, int32_t* branch, float* hit_p, float* normal, float* strength_out,

@@ -132,6 +132,25 @@ def test_render_small_capacity_equal(room):
     assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("steps", [1, 16])
+def test_step_traversal_renders_the_same_bits(spheres, steps):
+    """Step-at-a-time traversal (trav_steps > 0) renders the same bits as
+    the leaf-at-a-time kernel."""
+    _, gpu, _ = spheres
+    a = _render(gpu, S.ROOM_CAM, 48, 40, 1, 4, 6, (0.1, 0.1, 0.1), seed=31)
+    t0 = gpu.tuning()
+    t = gpu.tuning()
+    t.trav_steps = steps
+    gpu.set_tuning(t)
+    try:
+        b = _render(gpu, S.ROOM_CAM, 48, 40, 1, 4, 6, (0.1, 0.1, 0.1), seed=31)
+    finally:
+        gpu.set_tuning(t0)
+    assert np.array_equal(a[1], b[1])
+    for k in ("intersect_queries", "nodes_visited", "leaves_visited", "triangle_tests"):
+        assert a[2][k] == b[2][k], k
+
+
 def test_render_right_after_upload(spheres):
     """A render issued immediately after hpt_scene_create sees the whole
     scene: the same bits as a render on a scene uploaded long before (the

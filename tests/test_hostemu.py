@@ -50,6 +50,20 @@ def test_traversal_matches_oracle(pair, kind, smem):
     _same_hits(cs.intersect(o, d), got)
 
 
+@pytest.mark.parametrize("kind", ["camera", "pano", "random"])
+def test_step_traversal_matches_leaf_traversal(pair, kind):
+    """trav_step (one unit of work per call) gives the oracle's hits and the
+    same per-ray work as trav_leaf."""
+    cs, em = pair
+    o, d = _rays(kind)
+    a = em.intersect(o, d, smem_nodes=2048)
+    b = em.intersect(o, d, smem_nodes=2048, step=True)
+    assert b["err"][0] == 0, b["err"]
+    _same_hits(cs.intersect(o, d), b)
+    assert np.array_equal(a["node"], b["node"])
+    assert np.array_equal(a["counts"], b["counts"])
+
+
 def test_hinted_secondary_rays_match_oracle(pair):
     """Secondary rays started from the leaf of the previous hit (the kernels'
     start-leaf hint) find the same closest hit as a traversal from the root."""
@@ -67,6 +81,9 @@ def test_hinted_secondary_rays_match_oracle(pair):
         hinted = em.intersect(o2, nd, hints=first["node"][h], smem_nodes=2048)
         assert hinted["err"][0] == 0, hinted["err"]
         _same_hits(ref, hinted)
+        stepped = em.intersect(o2, nd, hints=first["node"][h], smem_nodes=2048, step=True)
+        assert stepped["err"][0] == 0, stepped["err"]
+        _same_hits(ref, stepped)
         plain = em.intersect(o2, nd)
         # a hint never costs more node visits than starting at the root
         assert hinted["counts"][0] <= plain["counts"][0]
