@@ -130,23 +130,25 @@ __device__ __forceinline__ void count_queries(DevSlot* slots, bool alive, int sl
 }
 
 // Warp-level reduction of the per-lane query and work counters.
-__device__ __forceinline__ void flush_counts(DevCtrl* c, unsigned long long q, TravCount n) {
+__device__ __forceinline__ void flush_counts(DevCtrl* c, unsigned long long q, TravCount lane) {
+  unsigned long long nodes = lane.nodes, leaves = lane.leaves, tris = lane.tris,
+                     repeats = lane.repeats;
   for (int o = 16; o > 0; o >>= 1) {
     q += __shfl_down_sync(kFull, q, o);
-    n.nodes += __shfl_down_sync(kFull, n.nodes, o);
-    n.leaves += __shfl_down_sync(kFull, n.leaves, o);
-    n.tris += __shfl_down_sync(kFull, n.tris, o);
-    n.repeats += __shfl_down_sync(kFull, n.repeats, o);
+    nodes += __shfl_down_sync(kFull, nodes, o);
+    leaves += __shfl_down_sync(kFull, leaves, o);
+    tris += __shfl_down_sync(kFull, tris, o);
+    repeats += __shfl_down_sync(kFull, repeats, o);
   }
   if ((threadIdx.x & 31) == 0 && q) {
 #ifdef HPT_DEVICE_CHECKS
     atomicAdd(&c->chk_isect_done, (int)q);
 #endif
     atomicAdd(&c->isect_queries, q);
-    atomicAdd(&c->nodes_visited, n.nodes);
-    atomicAdd(&c->leaves_visited, n.leaves);
-    atomicAdd(&c->tri_tests, n.tris);
-    atomicAdd(&c->tri_repeats, n.repeats);
+    atomicAdd(&c->nodes_visited, nodes);
+    atomicAdd(&c->leaves_visited, leaves);
+    atomicAdd(&c->tri_tests, tris);
+    atomicAdd(&c->tri_repeats, repeats);
   }
 }
 
@@ -207,7 +209,7 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
   TravState st;
   int slot = 0;
   int64_t ray = 0;
-  unsigned long long queries = 0;
+  uint32_t queries = 0;  // this lane's queries in this launch
   TravCount cnt;
   while (true) {
     const unsigned idle = __ballot_sync(kFull, !active);
@@ -450,7 +452,7 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
   StepState ss;
   int item = 0;   // index in the intersect queue; the payload is reloaded at the end
   int slot = 0;
-  unsigned long long queries = 0;
+  uint32_t queries = 0;  // this lane's queries in this launch
   TravCount cnt;
   while (true) {
     const unsigned idle = __ballot_sync(kFull, !active);
@@ -575,6 +577,8 @@ const IsectVariant kIsectVariants[] = {
     {128, 6, k_isect<128, 6, false>, k_isect<128, 6, true>, k_primary<128, 6>},
     {128, 7, k_isect<128, 7, false>, k_isect<128, 7, true>, k_primary<128, 7>},
     {128, 8, k_isect<128, 8, false>, k_isect<128, 8, true>, k_primary<128, 8>},
+    {128, 9, k_isect<128, 9, false>, k_isect<128, 9, true>, k_primary<128, 9>},
+    {128, 10, k_isect<128, 10, false>, k_isect<128, 10, true>, k_primary<128, 10>},
     {256, 2, k_isect<256, 2, false>, k_isect<256, 2, true>, k_primary<256, 2>},
     {256, 3, k_isect<256, 3, false>, k_isect<256, 3, true>, k_primary<256, 3>},
 };
@@ -661,11 +665,11 @@ hpt_tuning default_tuning() {
   hpt_tuning t;
   memset(&t, 0, sizeof t);
   // From the tuning sweep on the 61k-triangle spheres frame (512x512, 64 spp):
-  // step-at-a-time traversal, 24 units per refill check, 7 blocks of 128 per
-  // SM, no shared-node prefix.
+  // step-at-a-time traversal, 24 units per refill check, 8 blocks of 128 per
+  // SM (64 registers), no shared-node prefix.
   t.capacity = 1 << 22;
   t.isect_block = 128;
-  t.isect_min_blocks = 7;
+  t.isect_min_blocks = 8;
   t.shade_block = 256;
   t.refill_chunk = 4;
   t.smem_nodes = 0;

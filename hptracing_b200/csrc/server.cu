@@ -490,7 +490,7 @@ extern "C" hpt_status hpt_autotune(hpt_scene* scene, const hpt_camera* camera,
     void (*apply)(hpt_tuning&, int, int);
   };
   const Knob knobs[] = {
-      {{{128, 5}, {128, 6}, {128, 7}, {128, 8}, {256, 2}, {256, 3}},
+      {{{128, 5}, {128, 6}, {128, 7}, {128, 8}, {128, 9}, {128, 10}, {256, 2}, {256, 3}},
        [](hpt_tuning& t, int a, int b) {
          t.isect_block = a;
          t.isect_min_blocks = b;

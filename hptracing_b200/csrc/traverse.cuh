@@ -71,6 +71,13 @@ HPT_HD bool mt_test(const Ray& r, const float4 A, const float4 E1,
   return t > 0.f;
 }
 
+// Entries of the per-ray triangle mailbox (a performance knob only: a
+// repeated triangle that misses the mailbox is simply tested again).
+#ifndef HPT_MAILBOX
+#define HPT_MAILBOX 2
+#endif
+constexpr int kMailbox = HPT_MAILBOX;
+
 // Traversal state of one ray; lives in registers so a lane can be
 // refilled with a new ray between leaves.
 struct TravState {
@@ -82,15 +89,16 @@ struct TravState {
   int32_t steps;
   int32_t best_node;     // leaf node where the best hit was found
   Hit best;
-  // The last four triangles tested and their Moller-Trumbore t (-1 = miss):
-  // the reference tree repeats a triangle in every leaf it straddles.
-  int32_t mb_id[4];
-  float mb_t[4];
+  // The last kMailbox triangles tested and their Moller-Trumbore t (-1 =
+  // miss): the reference tree repeats a triangle in every leaf it straddles.
+  int32_t mb_id[kMailbox];
+  float mb_t[kMailbox];
 };
 
-// Work counters of one lane (summed over the rays it traced).
+// Work counters of one lane over one kernel launch (summed per warp in 64
+// bits when the launch ends; they feed statistics only).
 struct TravCount {
-  unsigned long long nodes = 0, leaves = 0, tris = 0, repeats = 0;
+  uint32_t nodes = 0, leaves = 0, tris = 0, repeats = 0;
 };
 
 // Starts a query. start_node (>= 0) names a leaf node the origin is
@@ -107,7 +115,7 @@ HPT_HD void trav_init(const DevScene& s, const Ray& r, TravState& st,
   st.steps = 0;
   st.node = -1;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
+  for (int k = 0; k < kMailbox; ++k) {
     st.mb_id[k] = -1;
     st.mb_t[k] = -1.f;
   }
@@ -235,12 +243,12 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, const uint2* smem,
       bool tested = false;
       int slot = -1;
 #pragma unroll
-      for (int m = 0; m < 4; ++m)
+      for (int m = 0; m < kMailbox; ++m)
         if (st.mb_id[m] == id) slot = m;
       if (slot >= 0) {
         ++cnt.repeats;
 #pragma unroll
-        for (int m = 0; m < 4; ++m)
+        for (int m = 0; m < kMailbox; ++m)
           if (m == slot) t = st.mb_t[m];
       } else {
         ++cnt.tris;
@@ -248,10 +256,13 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, const uint2* smem,
         const float4 A = ldg(rec), E1 = ldg(rec + 1), E2 = ldg(rec + 2);
         if (!mt_test(r, A, E1, E2, t, u, v)) t = -1.f;
         tested = true;
-        st.mb_id[3] = st.mb_id[2]; st.mb_t[3] = st.mb_t[2];
-        st.mb_id[2] = st.mb_id[1]; st.mb_t[2] = st.mb_t[1];
-        st.mb_id[1] = st.mb_id[0]; st.mb_t[1] = st.mb_t[0];
-        st.mb_id[0] = id; st.mb_t[0] = t;
+#pragma unroll
+        for (int m = kMailbox - 1; m > 0; --m) {
+          st.mb_id[m] = st.mb_id[m - 1];
+          st.mb_t[m] = st.mb_t[m - 1];
+        }
+        st.mb_id[0] = id;
+        st.mb_t[0] = t;
       }
       if (t > 0.f &&
           (st.best.rec < 0 || t < st.best.t || (t == st.best.t && j < st.best.rec))) {
@@ -404,12 +415,12 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, StepState& ss, const uin
     bool tested = false;
     int slot = -1;
 #pragma unroll
-    for (int m = 0; m < 4; ++m)
+    for (int m = 0; m < kMailbox; ++m)
       if (st.mb_id[m] == id) slot = m;
     if (slot >= 0) {
       ++cnt.repeats;
 #pragma unroll
-      for (int m = 0; m < 4; ++m)
+      for (int m = 0; m < kMailbox; ++m)
         if (m == slot) t = st.mb_t[m];
     } else {
       ++cnt.tris;
@@ -417,10 +428,13 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, StepState& ss, const uin
       const float4 A = ldg(rec), E1 = ldg(rec + 1), E2 = ldg(rec + 2);
       if (!mt_test(r, A, E1, E2, t, u, v)) t = -1.f;
       tested = true;
-      st.mb_id[3] = st.mb_id[2]; st.mb_t[3] = st.mb_t[2];
-      st.mb_id[2] = st.mb_id[1]; st.mb_t[2] = st.mb_t[1];
-      st.mb_id[1] = st.mb_id[0]; st.mb_t[1] = st.mb_t[0];
-      st.mb_id[0] = id; st.mb_t[0] = t;
+#pragma unroll
+      for (int m = kMailbox - 1; m > 0; --m) {
+        st.mb_id[m] = st.mb_id[m - 1];
+        st.mb_t[m] = st.mb_t[m - 1];
+      }
+      st.mb_id[0] = id;
+      st.mb_t[0] = t;
     }
     if (t > 0.f && (st.best.rec < 0 || t < st.best.t || (t == st.best.t && j < st.best.rec))) {
       if (ss.pierced < 0) {
