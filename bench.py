@@ -31,6 +31,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 W_RES, H_RES, SPP, DEPTH = 512, 512, 64, 8
+BG = (0.0, 0.0, 0.0)  # the terrain frame adds a constant environment term of 0.2
 WORKLOAD = "spheres64_61k_tris_512x512_spp64_d8"
 
 
@@ -47,6 +48,9 @@ def parse():
     # Extra workloads (one JSON line each): the 32-job mixed batch, batched
     # vs one job at a time; the Poisson serving stream.
     ap.add_argument("--mode", default="frame", choices=["frame", "batch", "serve"])
+    ap.add_argument("--scene", default="spheres", choices=["spheres", "terrain"],
+                    help="frame: the 61k-triangle spheres frame (headline) or the "
+                         "2.4M-triangle terrain at 1920x1080, 256 spp")
     ap.add_argument("--rate", default="50", help="serve: requests per second (comma list)")
     ap.add_argument("--duration", type=float, default=4.0, help="serve: seconds of arrivals")
     ap.add_argument("--serve-capacity", type=int, default=1 << 20,
@@ -173,9 +177,16 @@ def profiled_traffic():
     return None
 
 
+SCENE = "spheres"
+
+
 def make_scene():
     import hptracing_b200 as H
     from tests import scenes as S
+    if SCENE == "terrain":
+        mesh = H.Mesh.generate(2, seed=2)
+        nodes, leaf = H.build_kdtree(mesh.points, mesh.triangles)
+        return mesh, nodes, leaf, S.terrain_cam(W_RES / H_RES)
     mesh, nodes, leaf = S.make_scene(1, seed=1)
     return mesh, nodes, leaf, S.ROOM_CAM
 
@@ -200,10 +211,10 @@ def cpu_baseline(mesh, nodes, leaf, cam, kind):
     threads = os.cpu_count() or 1
     t0 = time.perf_counter()
     if kind == "reference":
-        _, _, counts = cs.refcl_render(cam, W_RES, H_RES, 1, 1, (0, 0, 0), 1, DEPTH, 0, 1.0,
+        _, _, counts = cs.refcl_render(cam, W_RES, H_RES, 1, 1, BG, 1, DEPTH, 0, 1.0,
                                        seed=1, threads=threads)
     else:
-        _, _, counts = cs.render(cam, W_RES, H_RES, 1, 1, (0, 0, 0), 1, DEPTH, 0, seed=1,
+        _, _, counts = cs.render(cam, W_RES, H_RES, 1, 1, BG, 1, DEPTH, 0, seed=1,
                                  rng_mode=0, threads=threads)
     dt = time.perf_counter() - t0
     return {"value": counts[0] / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": kind,
@@ -473,7 +484,7 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, args):
 
 
 def main():
-    global W_RES, H_RES, SPP, WORKLOAD
+    global W_RES, H_RES, SPP, WORKLOAD, SCENE, BG
     args = parse()
     if args.mode == "batch":
         run_batch(args)
@@ -481,10 +492,17 @@ def main():
     if args.mode == "serve":
         run_serve(args)
         return
+    if args.scene == "terrain":
+        SCENE = "terrain"
+        W_RES, H_RES, SPP = 1920, 1080, 256
+        BG = (0.2, 0.2, 0.2)
+        WORKLOAD = "terrain_2.4M_tris_1920x1080_spp256_d8"
     if args.res or args.spp:
-        W_RES = H_RES = args.res or W_RES
+        if args.res:
+            H_RES = args.res * H_RES // W_RES
+            W_RES = args.res
         SPP = args.spp or SPP
-        WORKLOAD = "profiling_case_%dx%d_spp%d_d%d" % (W_RES, H_RES, SPP, DEPTH)
+        WORKLOAD = "profiling_case_%s_%dx%d_spp%d_d%d" % (SCENE, W_RES, H_RES, SPP, DEPTH)
     if args.impl == "reference":
         run_reference(args)
         return
@@ -505,7 +523,7 @@ def main():
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
 
     def frame(i):
-        p = H.make_params(W_RES, H_RES, 1, 1, (0, 0, 0), SPP, DEPTH, 0, 1.0, 1000 + i)
+        p = H.make_params(W_RES, H_RES, 1, 1, BG, SPP, DEPTH, 0, 1.0, 1000 + i)
         flush.zero_()
         torch.cuda.synchronize()
         barrier(world)

@@ -198,7 +198,8 @@ __device__ void schedule(const EngineParams& P) {
 // ---------------------------------------------------------------------------
 // Primary pass: raygen + closest hit, lanes refilled from a global counter.
 // ---------------------------------------------------------------------------
-template <int BS, int MINB>
+// kStep: step-at-a-time traversal as in k_isect.
+template <int BS, int MINB, bool kStep>
 __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
   extern __shared__ uint2 snodes[];
   const int n_smem = stage_nodes(P, snodes);
@@ -207,6 +208,7 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
   const int64_t total = P.prim_prefix[P.prim_n];
   bool active = false;
   TravState st;
+  StepState ss;
   int slot = 0;
   int64_t ray = 0;
   uint32_t queries = 0;  // this lane's queries in this launch
@@ -233,6 +235,7 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
             const f3 d = J.pano ? pano_dir(x, y, J.vr_x_shift, J.ny)
                                 : pinhole_dir(J.top, J.right, J.width, J.height, x, y, J.nx, J.ny);
             trav_init(J.scene, Ray{mk(J.view_p[0], J.view_p[1], J.view_p[2]), d}, st);
+            if (kStep) step_init(ss);
             active = true;
             ++queries;
           }
@@ -241,7 +244,18 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
     }
     if (__ballot_sync(kFull, active) == 0) break;
     bool finished = false;
-    if (active) finished = trav_leaf(P.jobs[slot].scene, st, snodes, n_smem, &c->err, cnt);
+    if (active) {
+      if constexpr (kStep) {
+        const DevScene& sc = P.jobs[slot].scene;
+        for (int u = 0; u < P.trav_steps; ++u)
+          if (trav_step(sc, st, ss, snodes, n_smem, &c->err, cnt)) {
+            finished = true;
+            break;
+          }
+      } else {
+        finished = trav_leaf(P.jobs[slot].scene, st, snodes, n_smem, &c->err, cnt);
+      }
+    }
     if (finished) {
       const DevJob& J = P.jobs[slot];
       if (st.best.rec >= 0) {
@@ -571,16 +585,17 @@ struct IsectVariant {
   void (*isect)(EngineParams);       // one leaf per round
   void (*isect_step)(EngineParams);  // step-at-a-time
   void (*primary)(EngineParams);
+  void (*primary_step)(EngineParams);
 };
 const IsectVariant kIsectVariants[] = {
-    {128, 5, k_isect<128, 5, false>, k_isect<128, 5, true>, k_primary<128, 5>},
-    {128, 6, k_isect<128, 6, false>, k_isect<128, 6, true>, k_primary<128, 6>},
-    {128, 7, k_isect<128, 7, false>, k_isect<128, 7, true>, k_primary<128, 7>},
-    {128, 8, k_isect<128, 8, false>, k_isect<128, 8, true>, k_primary<128, 8>},
-    {128, 9, k_isect<128, 9, false>, k_isect<128, 9, true>, k_primary<128, 9>},
-    {128, 10, k_isect<128, 10, false>, k_isect<128, 10, true>, k_primary<128, 10>},
-    {256, 2, k_isect<256, 2, false>, k_isect<256, 2, true>, k_primary<256, 2>},
-    {256, 3, k_isect<256, 3, false>, k_isect<256, 3, true>, k_primary<256, 3>},
+    {128, 5, k_isect<128, 5, false>, k_isect<128, 5, true>, k_primary<128, 5, false>, k_primary<128, 5, true>},
+    {128, 6, k_isect<128, 6, false>, k_isect<128, 6, true>, k_primary<128, 6, false>, k_primary<128, 6, true>},
+    {128, 7, k_isect<128, 7, false>, k_isect<128, 7, true>, k_primary<128, 7, false>, k_primary<128, 7, true>},
+    {128, 8, k_isect<128, 8, false>, k_isect<128, 8, true>, k_primary<128, 8, false>, k_primary<128, 8, true>},
+    {128, 9, k_isect<128, 9, false>, k_isect<128, 9, true>, k_primary<128, 9, false>, k_primary<128, 9, true>},
+    {128, 10, k_isect<128, 10, false>, k_isect<128, 10, true>, k_primary<128, 10, false>, k_primary<128, 10, true>},
+    {256, 2, k_isect<256, 2, false>, k_isect<256, 2, true>, k_primary<256, 2, false>, k_primary<256, 2, true>},
+    {256, 3, k_isect<256, 3, false>, k_isect<256, 3, true>, k_primary<256, 3, false>, k_primary<256, 3, true>},
 };
 constexpr int kNumIsectVariants = sizeof(kIsectVariants) / sizeof(kIsectVariants[0]);
 
@@ -871,6 +886,8 @@ static hpt_status raise_smem_limits(int device) {
   const int bytes = kMaxSmemNodes * (int)sizeof(uint2);
   for (const IsectVariant& v : kIsectVariants) {
     HPT_CUDA(cudaFuncSetAttribute(v.primary, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    HPT_CUDA(cudaFuncSetAttribute(v.primary_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  bytes));
     HPT_CUDA(cudaFuncSetAttribute(v.isect, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     HPT_CUDA(cudaFuncSetAttribute(v.isect_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   bytes));
@@ -1050,7 +1067,10 @@ hpt_status Engine::admit(const std::vector<int>& slot_ids, const std::vector<Dev
                                A_leaf_, R, shared_scene);
   const size_t smem = (size_t)P.smem_nodes * sizeof(uint2);
   const IsectVariant& v = kIsectVariants[isect_variant()];
-  v.primary<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
+  if (P.trav_steps > 0)
+    v.primary_step<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
+  else
+    v.primary<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
   HPT_CUDA(cudaGetLastError());
   hpt_status s = set_order(order);  // synchronises: the staging is free again
   if (s != HPT_OK) return s;
