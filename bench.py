@@ -84,23 +84,13 @@ def barrier(world):
 
 
 def allreduce_max(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from hptracing_b200 import shard
+    return shard.allreduce_max(x, world, device="cuda")
 
 
 def allreduce_sum(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    from hptracing_b200 import shard
+    return shard.allreduce_sum(x, world, device="cuda")
 
 
 class ClockSampler:
@@ -294,10 +284,17 @@ def run_batch(args):
     import torch
     import hptracing_b200 as H
     from hptracing_b200 import build as hbuild
+    from hptracing_b200 import shard
     from tests import scenes as S
+    rank, world, local = dist_setup(args.gpus)
     hbuild.build()
-    torch.cuda.set_device(0)
-    jobs = c3_jobs()
+    torch.cuda.set_device(local)
+    all_jobs = c3_jobs()
+    # With N ranks each runs its share (longest job first onto the least
+    # loaded rank); the 32 jobs are the fixed total work (strong scaling).
+    table = shard.assign_jobs([shard.job_cost(j["res"] ** 2, j["spp"], j["depth"])
+                               for j in all_jobs], world)
+    jobs = [all_jobs[i] for i in table[rank]]
     t0 = time.perf_counter()
     built = []
     for j in jobs:
@@ -343,14 +340,25 @@ def run_batch(args):
 
     plain()
     batched()
+    barrier(world)
     q_p, ms_p, wall_p, acc_p = plain()
+    barrier(world)
     q_b, ms_b, wall_b, acc_b = batched()
     same = all(np.array_equal(a, b) for a, b in zip(acc_p, acc_b))
-    work = [j["res"] ** 2 * j["spp"] * j["depth"] for j in jobs]
+    q_p, q_b = allreduce_sum(q_p, world), allreduce_sum(q_b, world)
+    ms_p, ms_b = allreduce_max(ms_p, world), allreduce_max(ms_b, world)
+    wall_p, wall_b = allreduce_max(wall_p, world), allreduce_max(wall_b, world)
+    same = allreduce_sum(0.0 if same else 1.0, world) == 0.0
+    if rank != 0:
+        for sc, _, _, _ in built:
+            sc.close()
+        return
+    work = [j["res"] ** 2 * j["spp"] * j["depth"] for j in all_jobs]
     line = {
         "metric": "Mrays/s batched vs plain (C3, 32 mixed jobs)", "mode": "batch",
         "value": q_b / ms_b / 1e3, "unit": "Mrays/s", "plain": q_p / ms_p / 1e3,
-        "speedup": (q_b / ms_b) / (q_p / ms_p), "higher_is_better": True, "n_gpus": 1,
+        "speedup": (q_b / ms_b) / (q_p / ms_p), "higher_is_better": True, "n_gpus": world,
+        "scaling": "strong", "jobs_per_rank": [len(t) for t in table],
         "ms_batched": ms_b, "ms_plain": ms_p, "queries": q_b,
         "e2e": {"batched": q_b / wall_b / 1e6, "plain": q_p / wall_p / 1e6, "unit": "Mrays/s"},
         "accumulators_bit_identical": same,
@@ -359,7 +367,7 @@ def run_batch(args):
                    "isect_min_blocks": tune.isect_min_blocks, "refill": tune.refill_chunk,
                    "smem_nodes": tune.smem_nodes, "use_graph": tune.use_graph,
                    "trav_steps": tune.trav_steps},
-        "jobs": [dict(j, triangles=b[3]) for j, b in zip(jobs, built)],
+        "jobs": all_jobs,
         "scene_build_s": build_s, "dtype": "f32", "data": "synthetic (seeded scene families)"}
     print(json.dumps(line), flush=True)
     for sc, _, _, _ in built:
@@ -488,6 +496,9 @@ def main():
     args = parse()
     if args.mode == "batch":
         run_batch(args)
+        if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     if args.mode == "serve":
         run_serve(args)
