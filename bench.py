@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--duration", type=float, default=4.0, help="serve: seconds of arrivals")
     ap.add_argument("--serve-capacity", type=int, default=1 << 20,
                     help="serve: wavefront capacity (paths in flight)")
-    ap.add_argument("--large-pct", type=int, default=25,
+    ap.add_argument("--large-pct", type=int, default=10,
                     help="serve: in-flight cap of requests larger than the wavefront, %%")
     ap.add_argument("--terrain-n", type=int, default=1024,
                     help="serve: heightfield vertices per side of the large scenes")
@@ -441,6 +441,7 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, args):
     start = time.perf_counter()
     outstanding = {}
     lat = {"pose": [], "pano": []}
+    per_scene = {}
     samples = 0
     nxt = 0
     drain_cap = args.duration + 20.0
@@ -449,7 +450,7 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, args):
         while nxt < len(arrivals) and arrivals[nxt][0] <= now:
             _, kind, k, cam, p = arrivals[nxt]
             rid = server.submit(slots[k], S.hp_camera(cam), p)
-            outstanding[rid] = (kind, p)
+            outstanding[rid] = (kind, p, k)
             nxt += 1
         if not outstanding and nxt >= len(arrivals):
             break
@@ -460,8 +461,11 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, args):
             for rid in server.completed():
                 st, info = server.poll(rid)
                 if st == 0 and rid in outstanding:
-                    kind, p = outstanding.pop(rid)
+                    kind, p, k = outstanding.pop(rid)
                     lat[kind].append(info["done_ms"] - info["submit_ms"])
+                    per_scene.setdefault((kind, k), []).append(
+                        (info["done_ms"] - info["submit_ms"], info["admit_ms"] - info["submit_ms"],
+                         info["submit_ms"]))
                     samples += p.sample_x * p.sample_y * p.sample
         else:
             time.sleep(0.0005)
@@ -482,6 +486,10 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, args):
                               "p99_ms": pct(lat["pose"], 99)},
         "pano_2048x1024_64spp": {"n": len(lat["pano"]), "p50_ms": pct(lat["pano"], 50),
                                  "p99_ms": pct(lat["pano"], 99)},
+        "per_scene": {"%s/scene%d" % key: {
+            "n": len(v), "p50_ms": pct([x[0] for x in v], 50), "p99_ms": pct([x[0] for x in v], 99),
+            "max_ms": max(x[0] for x in v), "admit_wait_max_ms": max(x[1] for x in v),
+            "slowest_submitted_at_ms": max(v)[2]} for key, v in sorted(per_scene.items())},
         "Mrays_per_s": q / elapsed / 1e6, "Msamples_per_s": samples / elapsed / 1e6,
         "server": {"capacity": args.serve_capacity, "large_inflight_pct": args.large_pct,
                    "max_jobs": 64, "memory_budget": 16 << 30},

@@ -150,6 +150,9 @@ struct DevCtrl {
   int32_t chk_shade_done;
   int32_t chk_isect_done;
   int32_t chk_pad;
+  // Started-but-unfinished paths all capped slots (max_inflight > 0) may
+  // hold together (0 = no shared cap); host-written.
+  int64_t capped_budget;
 };
 
 // Fixed-point scale of the per-ray accumulators (2^32): integer sums are

@@ -167,6 +167,15 @@ __device__ void schedule(const EngineParams& P) {
   const int budget = P.capacity - c->nA;
   int n_new = 0, nq = 0;
   bool remaining = false;
+  // Paths the capped slots hold now, against their shared budget.
+  int64_t capped = 0;
+  if (c->capped_budget > 0)
+    for (int k = 0; k < c->n_order; ++k) {
+      const int s = P.order[k];
+      if (s < 0 || s >= P.num_slots) continue;
+      const DevSlot& S = P.slots[s];
+      if (S.active && S.max_inflight > 0) capped += S.cursor - (int64_t)S.done;
+    }
   for (int k = 0; k < c->n_order; ++k) {
     const int s = P.order[k];
     HPT_DCHECK(&c->err, s >= 0 && s < P.num_slots, 231, s, continue);
@@ -180,9 +189,13 @@ __device__ void schedule(const EngineParams& P) {
     // A capped job (e.g. a large request that must not crowd out the
     // latency-sensitive ones behind it) keeps at most max_inflight paths
     // started and unfinished.
-    if (S.max_inflight > 0) grant = min(grant, S.max_inflight - (S.cursor - (int64_t)S.done));
+    if (S.max_inflight > 0) {
+      grant = min(grant, S.max_inflight - (S.cursor - (int64_t)S.done));
+      if (c->capped_budget > 0) grant = min(grant, c->capped_budget - capped);
+    }
     const int a = (int)grant;
     if (a <= 0) continue;
+    if (S.max_inflight > 0) capped += a;
     S.alloc = a;
     P.quota_slot[nq] = s;
     P.quota_prefix[nq] = n_new;
@@ -1160,6 +1173,14 @@ hpt_status Engine::read_state(std::vector<DevSlot>& slots, DevCtrl* ctrl) {
   HPT_CUDA(cudaStreamSynchronize(stream));
   std::copy(slots_host_, slots_host_ + slots_, slots.begin());
   *ctrl = *ctrl_host_;
+  return HPT_OK;
+}
+
+hpt_status Engine::set_capped_budget(int64_t paths) {
+  ctrl_host_->capped_budget = paths;
+  HPT_CUDA(cudaMemcpyAsync(&ctrl_->capped_budget, &ctrl_host_->capped_budget, sizeof(int64_t),
+                           cudaMemcpyHostToDevice, stream));
+  HPT_CUDA(cudaStreamSynchronize(stream));
   return HPT_OK;
 }
 

@@ -86,6 +86,8 @@ class Engine {
   // Synchronous read-back of the slot table / control block.
   hpt_status read_slots(std::vector<DevSlot>& out);
   hpt_status read_ctrl(DevCtrl* out);
+  // Shared in-flight budget of the capped slots (reset_ctrl clears it).
+  hpt_status set_capped_budget(int64_t paths);
   hpt_status read_state(std::vector<DevSlot>& slots, DevCtrl* ctrl);  // one sync
   void reset_ctrl();
   DevCtrl* ctrl_dev() const { return ctrl_; }

@@ -214,6 +214,14 @@ hpt_status hpt_server_create(const hpt_server_config* config, hpt_server** out) 
     if (st != HPT_OK) return st;
     s->engine->reset_ctrl();
     HPT_CUDA(cudaStreamSynchronize(s->engine->stream));
+    // All large requests together keep at most large_inflight_pct of the
+    // wavefront in flight, however many of them are running.
+    const int pct = config->large_inflight_pct;
+    if (pct > 0 && pct < 100) {
+      st = s->engine->set_capped_budget(
+          std::max<int64_t>(1024, (int64_t)config->capacity * pct / 100));
+      if (st != HPT_OK) return st;
+    }
     s->slot_req.assign(config->max_jobs, 0);
     *out = s.release();
     return HPT_OK;

@@ -389,9 +389,9 @@ typedef struct hpt_server_config {
   int64_t memory_budget;      /* bytes of per-request device state        */
   int32_t capacity;           /* paths in flight shared by all requests   */
   int32_t progressive;        /* stream partial accumulations             */
-  /* A request with more paths (rays x spp) than `capacity` keeps at most
-   * this percentage of `capacity` in flight, so it cannot crowd out the
-   * smaller requests admitted after it (0 or 100 = no cap). */
+  /* Requests with more paths (rays x spp) than `capacity` keep together at
+   * most this percentage of `capacity` in flight, so they cannot crowd out
+   * the smaller requests admitted after them (0 or 100 = no cap). */
   int32_t large_inflight_pct;
   int32_t reserved[3];
 } hpt_server_config;
