@@ -175,3 +175,25 @@ def test_trace_runner_shim(room):
                24, 1, 1, (0, 0, 0), sample=4, depth=4)
     assert pixels.reshape(24, 32, 4)[..., :3].mean() > 5
     assert (pixels.reshape(24, 32, 4)[..., 3] == 0).all()
+
+
+def test_cli_replays_gui_camera_keys(built, tmp_path):
+    """hptracing --keys: the first frame plus one per key that re-renders in
+    the reference GUI ('[' only halves the step)."""
+    import os
+    import subprocess
+    cli = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                       "hptracing_b200", "hptracing")
+    out = str(tmp_path / "cam.ppm")
+    r = subprocess.run([cli, "-i", "generated:0", "-o", out, "--width", "48", "--height", "32",
+                        "-s", "2", "-d", "4", "--view", "0.5,0.5,-1.4", "--right", "-1,0,0",
+                        "--angle", "0.73", "--keys", "a[d"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    frames = []
+    for k in range(3):
+        path = str(tmp_path / ("cam_%03d.ppm" % k))
+        data = open(path, "rb").read()
+        assert data.startswith(b"P6\n48 32\n255\n")
+        frames.append(np.frombuffer(data[len(b"P6\n48 32\n255\n"):], np.uint8))
+    assert not os.path.exists(str(tmp_path / "cam_003.ppm"))
+    assert np.abs(frames[1].astype(int) - frames[0].astype(int)).mean() > 1.0
