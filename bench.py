@@ -53,10 +53,13 @@ def parse():
                          "2.4M-triangle terrain at 1920x1080, 256 spp")
     ap.add_argument("--rate", default="50", help="serve: requests per second (comma list)")
     ap.add_argument("--duration", type=float, default=4.0, help="serve: seconds of arrivals")
-    ap.add_argument("--serve-capacity", type=int, default=1 << 20,
-                    help="serve: wavefront capacity (paths in flight)")
-    ap.add_argument("--large-pct", type=int, default=10,
-                    help="serve: in-flight cap of requests larger than the wavefront, %%")
+    ap.add_argument("--serve-capacity", default=str(1 << 20),
+                    help="serve: wavefront capacity (paths in flight; comma list)")
+    ap.add_argument("--large-pct", default="10",
+                    help="serve: in-flight cap of the requests larger than the wavefront, "
+                         "%% (comma list)")
+    ap.add_argument("--depth-ahead", default="1",
+                    help="serve: iterations queued ahead of the host (comma list)")
     ap.add_argument("--terrain-n", type=int, default=1024,
                     help="serve: heightfield vertices per side of the large scenes")
     return ap.parse_args()
@@ -400,15 +403,18 @@ def run_serve(args):
         del mesh, nodes, leaf
     build_s = time.perf_counter() - t0
     for rate in [float(x) for x in str(args.rate).split(",")]:
-        serve_stream(H, S, scenes, cams, tris, build_s, rate, args)
+        for cap in [int(x) for x in str(args.serve_capacity).split(",")]:
+            for pct in [int(x) for x in str(args.large_pct).split(",")]:
+                for ahead in [int(x) for x in str(args.depth_ahead).split(",")]:
+                    serve_stream(H, S, scenes, cams, tris, build_s, rate, args, cap, pct, ahead)
     for sc in scenes:
         sc.close()
 
 
-def serve_stream(H, S, scenes, cams, tris, build_s, rate, args):
+def serve_stream(H, S, scenes, cams, tris, build_s, rate, args, capacity, large_pct, ahead):
     """One Poisson stream at `rate` requests/s against a fresh server."""
-    server = H.Server(max_jobs=64, memory_budget=16 << 30, capacity=args.serve_capacity,
-                      large_inflight_pct=args.large_pct)
+    server = H.Server(max_jobs=64, memory_budget=16 << 30, capacity=capacity,
+                      large_inflight_pct=large_pct, pipeline_depth=ahead, keep_accum=0)
     slots = [server.add_scene(s) for s in scenes]
     rng = np.random.default_rng(0x48505404 + int(rate))
     arrivals, t = [], 0.0
@@ -442,6 +448,7 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, args):
     outstanding = {}
     lat = {"pose": [], "pano": []}
     per_scene = {}
+    pumps, gaps, last_pump_end = [], [], None
     samples = 0
     nxt = 0
     drain_cap = args.duration + 20.0
@@ -457,7 +464,12 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, args):
         if now > drain_cap:
             break
         if outstanding:
+            tp = time.perf_counter()
+            if last_pump_end is not None:
+                gaps.append(((tp - start) * 1e3, (tp - last_pump_end) * 1e3))
             server.pump(1)
+            last_pump_end = time.perf_counter()
+            pumps.append(((tp - start) * 1e3, (last_pump_end - tp) * 1e3))
             for rid in server.completed():
                 st, info = server.poll(rid)
                 if st == 0 and rid in outstanding:
@@ -490,9 +502,13 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, args):
             "n": len(v), "p50_ms": pct([x[0] for x in v], 50), "p99_ms": pct([x[0] for x in v], 99),
             "max_ms": max(x[0] for x in v), "admit_wait_max_ms": max(x[1] for x in v),
             "slowest_submitted_at_ms": max(v)[2]} for key, v in sorted(per_scene.items())},
+        "host_loop": {"pumps": len(pumps),
+                      "pump_ms_p50": pct([x[1] for x in pumps], 50),
+                      "slowest_pumps_at_ms": sorted(pumps, key=lambda x: -x[1])[:5],
+                      "slowest_gaps_at_ms": sorted(gaps, key=lambda x: -x[1])[:3]},
         "Mrays_per_s": q / elapsed / 1e6, "Msamples_per_s": samples / elapsed / 1e6,
-        "server": {"capacity": args.serve_capacity, "large_inflight_pct": args.large_pct,
-                   "max_jobs": 64, "memory_budget": 16 << 30},
+        "server": {"capacity": capacity, "large_inflight_pct": large_pct,
+                   "pipeline_depth": ahead, "max_jobs": 64, "memory_budget": 16 << 30},
         "scene_triangles": tris, "scene_build_s": build_s, "clocks": clocks,
         "dtype": "f32", "data": "synthetic (seeded scenes, seeded Poisson stream)"}
     print(json.dumps(line), flush=True)

@@ -437,9 +437,9 @@ class Server:
     """Continuous-batching render server (hpt_server)."""
 
     def __init__(self, device=0, max_jobs=64, memory_budget=8 << 30, capacity=1 << 22,
-                 progressive=0, large_inflight_pct=0):
+                 progressive=0, large_inflight_pct=0, pipeline_depth=0, keep_accum=1):
         cfg = ServerConfig(device, max_jobs, memory_budget, capacity, progressive,
-                           large_inflight_pct)
+                           large_inflight_pct, pipeline_depth, keep_accum)
         h = C.c_void_p()
         check(lib().hpt_server_create(C.byref(cfg), C.byref(h)))
         self._h = h

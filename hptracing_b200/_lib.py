@@ -98,7 +98,8 @@ class Tuning(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("device", i32), ("max_jobs", i32), ("memory_budget", i64), ("capacity", i32),
-                ("progressive", i32), ("large_inflight_pct", i32), ("reserved", i32 * 3)]
+                ("progressive", i32), ("large_inflight_pct", i32), ("pipeline_depth", i32),
+                ("keep_accum", i32), ("reserved", i32 * 1)]
 
 
 class RequestInfo(C.Structure):

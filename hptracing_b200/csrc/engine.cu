@@ -793,6 +793,12 @@ Engine::~Engine() {
   if (done_host_) HPT_SOFT(cudaFreeHost(done_host_));
   if (pool_) HPT_SOFT(cudaMemPoolDestroy(pool_));
   if (graph_exec_) HPT_SOFT(cudaGraphExecDestroy(graph_exec_));
+  for (StagingSet& st : staging_) {
+    HPT_SOFT(cudaFreeHost(st.jobs));
+    HPT_SOFT(cudaFreeHost(st.i32));
+    HPT_SOFT(cudaFreeHost(st.i64));
+    if (st.ev) HPT_SOFT(cudaEventDestroy(st.ev));
+  }
   if (stream) HPT_SOFT(cudaStreamDestroy(stream));
 }
 
@@ -1092,6 +1098,114 @@ hpt_status Engine::admit(const std::vector<int>& slot_ids, const std::vector<Dev
   return HPT_OK;
 }
 
+// --- Asynchronous uploads (serving loop) ------------------------------------
+hpt_status Engine::next_staging(StagingSet** out) {
+  if (staging_slots_ != slots_) {
+    for (StagingSet& st : staging_) {
+      if (st.ev) HPT_CUDA(cudaEventSynchronize(st.ev));
+      HPT_SOFT(cudaFreeHost(st.jobs));
+      HPT_SOFT(cudaFreeHost(st.i32));
+      HPT_SOFT(cudaFreeHost(st.i64));
+      st.jobs = nullptr;
+      st.i32 = nullptr;
+      st.i64 = nullptr;
+    }
+    staging_slots_ = 0;
+    const size_t n = (size_t)slots_;
+    for (StagingSet& st : staging_) {
+      HPT_CUDA(cudaMallocHost(&st.jobs, n * sizeof(DevJob)));
+      HPT_CUDA(cudaMallocHost(&st.i32, (2 * n + 3) * sizeof(int32_t)));
+      HPT_CUDA(cudaMallocHost(&st.i64, (n + 1) * sizeof(int64_t)));
+      if (!st.ev) HPT_CUDA(cudaEventCreateWithFlags(&st.ev, cudaEventDisableTiming));
+    }
+    staging_slots_ = slots_;
+  }
+  StagingSet& st = staging_[staging_next_];
+  staging_next_ = (staging_next_ + 1) % kStagingRing;
+  // The set's previous copies were enqueued kStagingRing uploads ago; wait
+  // until they have run before overwriting their source.
+  HPT_CUDA(cudaEventSynchronize(st.ev));
+  *out = &st;
+  return HPT_OK;
+}
+
+hpt_status Engine::upload_order(const std::vector<int>& order, StagingSet& st) {
+  if ((int)order.size() > slots_) return fail(HPT_ERR_INVALID_ARGUMENT, "order larger than slots");
+  int32_t* stage = st.i32 + (slots_ + 1);
+  for (size_t k = 0; k < order.size(); ++k) stage[k] = order[k];
+  if (!order.empty())
+    HPT_CUDA(cudaMemcpyAsync(order_, stage, order.size() * sizeof(int32_t),
+                             cudaMemcpyHostToDevice, stream));
+  stage[slots_ + 1] = (int32_t)order.size();
+  HPT_CUDA(cudaMemcpyAsync(&ctrl_->n_order, &stage[slots_ + 1], sizeof(int32_t),
+                           cudaMemcpyHostToDevice, stream));
+  return HPT_OK;
+}
+
+hpt_status Engine::set_order_async(const std::vector<int>& order) {
+  StagingSet* st = nullptr;
+  hpt_status s = next_staging(&st);
+  if (s != HPT_OK) return s;
+  s = upload_order(order, *st);
+  if (s != HPT_OK) return s;
+  HPT_CUDA(cudaEventRecord(st->ev, stream));
+  return HPT_OK;
+}
+
+hpt_status Engine::admit_async(const std::vector<int>& slot_ids, const std::vector<DevJob>& jobs,
+                               const std::vector<int64_t>& rays, const std::vector<int>& order,
+                               const DevScene* shared_scene) {
+  const int n = (int)slot_ids.size();
+  if (n == 0) return set_order_async(order);
+  hpt_status s = query_occupancy();
+  if (s != HPT_OK) return s;
+  StagingSet* st = nullptr;
+  s = next_staging(&st);
+  if (s != HPT_OK) return s;
+  for (int k = 0; k < n; ++k) {
+    if (slot_ids[k] < 0 || slot_ids[k] >= slots_)
+      return fail(HPT_ERR_INVALID_ARGUMENT, "slot %d out of range", slot_ids[k]);
+    st->jobs[k] = jobs[k];
+    HPT_CUDA(cudaMemcpyAsync(jobs_ + slot_ids[k], st->jobs + k, sizeof(DevJob),
+                             cudaMemcpyHostToDevice, stream));
+  }
+  st->i64[0] = 0;
+  for (int k = 0; k < n; ++k) {
+    st->i32[k] = slot_ids[k];
+    st->i64[k + 1] = st->i64[k] + rays[k];
+  }
+  HPT_CUDA(cudaMemcpyAsync(prim_slot_, st->i32, n * sizeof(int32_t), cudaMemcpyHostToDevice,
+                           stream));
+  HPT_CUDA(cudaMemcpyAsync(prim_prefix_, st->i64, (n + 1) * sizeof(int64_t),
+                           cudaMemcpyHostToDevice, stream));
+  s = upload_order(order, *st);
+  if (s != HPT_OK) return s;
+  HPT_CUDA(cudaEventRecord(st->ev, stream));
+  float4* A[8] = {A_o_[0], A_d_[0], A_s_[0], A_r_[0], A_o_[1], A_d_[1], A_s_[1], A_r_[1]};
+  float4* R[4] = {R_o_, R_d_, R_s_, R_r_};
+  EngineParams P = make_params(*this, ctrl_, jobs_, slot_state_, slots_, order_, quota_slot_,
+                               quota_prefix_, prim_slot_, prim_prefix_, n, capacity_, A, A_tri_,
+                               A_leaf_, R, shared_scene);
+  const size_t smem = (size_t)P.smem_nodes * sizeof(uint2);
+  const IsectVariant& v = kIsectVariants[isect_variant()];
+  if (P.trav_steps > 0)
+    v.primary_step<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
+  else
+    v.primary<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
+  k_admit<<<1, 1, 0, stream>>>(P);
+  HPT_CUDA(cudaGetLastError());
+  return HPT_OK;
+}
+
+hpt_status Engine::read_state_async(DevSlot* slots, DevCtrl* ctrl, cudaEvent_t ev) {
+  if (slots_ > 0)
+    HPT_CUDA(cudaMemcpyAsync(slots, slot_state_, (size_t)slots_ * sizeof(DevSlot),
+                             cudaMemcpyDeviceToHost, stream));
+  HPT_CUDA(cudaMemcpyAsync(ctrl, ctrl_, sizeof(DevCtrl), cudaMemcpyDeviceToHost, stream));
+  HPT_CUDA(cudaEventRecord(ev, stream));
+  return HPT_OK;
+}
+
 hpt_status Engine::ensure_graph(const DevScene* shared_scene, int iterations) {
   const void* key_nodes = shared_scene ? (const void*)shared_scene->nodes : nullptr;
   if (graph_exec_ && graph_nodes_ == key_nodes && graph_capacity_ == capacity_ &&
@@ -1173,6 +1287,21 @@ hpt_status Engine::read_state(std::vector<DevSlot>& slots, DevCtrl* ctrl) {
   HPT_CUDA(cudaStreamSynchronize(stream));
   std::copy(slots_host_, slots_host_ + slots_, slots.begin());
   *ctrl = *ctrl_host_;
+  return HPT_OK;
+}
+
+hpt_status Engine::reserve_pool(size_t bytes) {
+  if (bytes == 0) return HPT_OK;
+  uint64_t keep = 0;
+  HPT_CUDA(cudaMemPoolGetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
+  if (keep < bytes) {
+    keep = bytes;
+    HPT_CUDA(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
+  void* p = nullptr;
+  HPT_CUDA(cudaMallocFromPoolAsync(&p, bytes, pool_, stream));
+  HPT_CUDA(cudaFreeAsync(p, stream));
+  HPT_CUDA(cudaStreamSynchronize(stream));
   return HPT_OK;
 }
 

@@ -77,6 +77,16 @@ class Engine {
                    const std::vector<int64_t>& rays, const std::vector<int>& order,
                    const DevScene* shared_scene);
   hpt_status set_order(const std::vector<int>& order);
+  // Asynchronous forms for a serving loop: the uploads go through a ring of
+  // pinned staging sets and nothing waits for the stream (only, rarely, for
+  // a staging set's previous copies to have run).
+  hpt_status admit_async(const std::vector<int>& slot_ids, const std::vector<DevJob>& jobs,
+                         const std::vector<int64_t>& rays, const std::vector<int>& order,
+                         const DevScene* shared_scene);
+  hpt_status set_order_async(const std::vector<int>& order);
+  // Enqueues a copy of the slot table and control block into pinned host
+  // memory and records ev after it.
+  hpt_status read_state_async(DevSlot* slots, DevCtrl* ctrl, cudaEvent_t ev);
   void launch_iteration(const DevScene* shared_scene, cudaEvent_t* ev3 = nullptr);
   // Captures `iterations` consecutive iterations into graph_exec_ (kept
   // until the queues, slots, shared scene or tuning change).
@@ -86,6 +96,10 @@ class Engine {
   // Synchronous read-back of the slot table / control block.
   hpt_status read_slots(std::vector<DevSlot>& out);
   hpt_status read_ctrl(DevCtrl* out);
+  // Maps `bytes` of device memory into the job-buffer pool now and keeps
+  // it there, so later job allocations do not map memory (which blocks the
+  // host) on their way.
+  hpt_status reserve_pool(size_t bytes);
   // Shared in-flight budget of the capped slots (reset_ctrl clears it).
   hpt_status set_capped_budget(int64_t paths);
   hpt_status read_state(std::vector<DevSlot>& slots, DevCtrl* ctrl);  // one sync
@@ -126,6 +140,17 @@ class Engine {
   std::vector<cudaEvent_t> pev_;  // profiling events, created on first use
   int32_t* done_host_ = nullptr;  // pinned drain flags (double-buffered)
   cudaMemPool_t pool_ = nullptr;  // per-job buffers
+  struct StagingSet {
+    DevJob* jobs = nullptr;
+    int32_t* i32 = nullptr;
+    int64_t* i64 = nullptr;
+    cudaEvent_t ev = nullptr;
+  };
+  static constexpr int kStagingRing = 8;
+  StagingSet staging_[kStagingRing];
+  int staging_next_ = 0, staging_slots_ = 0;
+  hpt_status next_staging(StagingSet** out);
+  hpt_status upload_order(const std::vector<int>& order, StagingSet& st);
   cudaGraphExec_t graph_exec_ = nullptr;
   const void* graph_nodes_ = nullptr;
   int graph_capacity_ = 0, graph_slots_ = 0, graph_iters_ = 0, graph_tuning_ = -1;

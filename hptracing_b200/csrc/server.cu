@@ -6,10 +6,18 @@
 // against device-resident scenes wait in a queue, are admitted as soon as a
 // slot and their device footprint (ray state, accumulators, image) fit,
 // share one wavefront with every request already running (smallest
-// remaining work first), and are resolved and copied back the pump after
-// their last path finishes. Random streams are keyed by (request seed, ray,
-// sample, bounce) and radiance is summed in fixed point, so a request's
-// image is bit-identical whether it runs alone or in any mix.
+// remaining work first), and are resolved and copied back when their last
+// path finishes. Random streams are keyed by (request seed, ray, sample,
+// bounce) and radiance is summed in fixed point, so a request's image is
+// bit-identical whether it runs alone or in any mix.
+//
+// The pump never waits for the GPU in the steady state: it keeps up to
+// `pipeline_depth` wavefront iterations queued, each followed by an
+// asynchronous copy of the slot table into a ring of pinned buffers; it
+// admits requests and updates the priority order through pinned staging
+// on the same stream; finished requests are resolved into pinned output
+// buffers and marked done when that copy's event has completed. A read-back
+// is only applied to requests admitted before it was recorded.
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -28,6 +36,22 @@
 
 using namespace hpt;
 
+// Diagnostic build only (-DHPT_SERVER_TRACE): report pump phases that take
+// longer than 20 ms on stderr.
+#ifdef HPT_SERVER_TRACE
+#define HPT_TRACE_BEGIN(name) const auto trace_t0_##name = std::chrono::steady_clock::now()
+#define HPT_TRACE_END(name)                                                                  \
+  do {                                                                                       \
+    const double ms = std::chrono::duration<double, std::milli>(                             \
+                          std::chrono::steady_clock::now() - trace_t0_##name)                \
+                          .count();                                                          \
+    if (ms > 20.0) fprintf(stderr, "hpt server: %s took %.1f ms\n", #name, ms);             \
+  } while (0)
+#else
+#define HPT_TRACE_BEGIN(name) (void)0
+#define HPT_TRACE_END(name) (void)0
+#endif
+
 namespace {
 
 enum RequestState { kQueued = 0, kRunning = 1, kDone = 2, kFailed = 3, kCancelled = 4 };
@@ -39,6 +63,9 @@ struct Request {
   int slot = -1;
   bool want_accum = true;
   bool cancel = false;
+  bool finishing = false;   // resolve and copy-back enqueued
+  cudaEvent_t fin_ev = nullptr;
+  uint64_t admit_seq = 0;   // iterations launched before its admission
   JobBuffers buf;
   int64_t footprint = 0;
   int64_t rays = 0;
@@ -47,9 +74,21 @@ struct Request {
   int64_t queries = 0;
   double submit_ms = 0, admit_ms = 0, done_ms = 0;
   hpt_status error = HPT_OK;
-  std::vector<uint8_t> rgba;
-  std::vector<float> accum;
+  uint8_t* rgba = nullptr;  // pinned, from the server's pool
+  float* accum = nullptr;
+  size_t rgba_bytes = 0, accum_bytes = 0;
 };
+
+// One asynchronous read-back of the slot table and control block.
+struct Readback {
+  DevSlot* slots = nullptr;  // pinned
+  DevCtrl* ctrl = nullptr;   // pinned
+  cudaEvent_t ev = nullptr;
+  uint64_t seq = 0;          // iterations launched before it was recorded
+  bool pending = false;
+};
+
+constexpr int kReadbacks = 8;
 
 }  // namespace
 
@@ -60,13 +99,18 @@ struct hpt_server {
   std::mutex mu;
   std::map<uint64_t, std::unique_ptr<Request>> reqs;
   std::deque<uint64_t> queue;
-  std::vector<uint64_t> slot_req;  // slot -> running request id, 0 = free
+  std::vector<uint64_t> slot_req;  // slot -> request id holding it, 0 = free
   int64_t used_bytes = 0;
   uint64_t next_id = 1;
   std::chrono::steady_clock::time_point t0;
-  std::vector<DevSlot> slot_view;
+  Readback rb[kReadbacks];
+  int rb_fill = 0, rb_drain = 0, rb_pending = 0;
+  uint64_t launched = 0;
+  int depth = 2;
   DevCtrl ctrl_view{};
   std::vector<uint64_t> finished_ids;  // since the last hpt_server_drain_completed
+  std::multimap<size_t, void*> pinned_pool;  // free pinned output buffers by size
+  std::vector<cudaEvent_t> event_pool;
   int64_t completed = 0;
   int64_t pumps = 0;
 
@@ -78,12 +122,18 @@ struct hpt_server {
     auto it = reqs.find(id);
     return it == reqs.end() ? nullptr : it->second.get();
   }
-  // Active slots, smallest remaining work first.
+  bool running() const {
+    for (size_t k = 0; k < slot_req.size(); ++k)
+      if (slot_req[k] && !reqs.at(slot_req[k])->finishing) return true;
+    return false;
+  }
+  // Slots still computing, smallest remaining work first.
   std::vector<int> order() const {
     std::vector<std::pair<int64_t, int>> v;
     for (size_t k = 0; k < slot_req.size(); ++k) {
       if (!slot_req[k]) continue;
       const Request* r = reqs.at(slot_req[k]).get();
+      if (r->finishing) continue;
       const int64_t total = r->paths >= 0 ? r->paths : r->rays * r->js.params.sample;
       v.push_back({total - r->done_paths, (int)k});
     }
@@ -92,12 +142,36 @@ struct hpt_server {
     for (auto& p : v) o.push_back(p.second);
     return o;
   }
+  hpt_status take_pinned(size_t bytes, void** out) {
+    auto it = pinned_pool.find(bytes);
+    if (it != pinned_pool.end()) {
+      *out = it->second;
+      pinned_pool.erase(it);
+      return HPT_OK;
+    }
+    HPT_CUDA(cudaMallocHost(out, bytes));
+    return HPT_OK;
+  }
+  void give_pinned(void* p, size_t bytes) {
+    if (p) pinned_pool.insert({bytes, p});
+  }
+  hpt_status take_event(cudaEvent_t* ev) {
+    if (!event_pool.empty()) {
+      *ev = event_pool.back();
+      event_pool.pop_back();
+      return HPT_OK;
+    }
+    HPT_CUDA(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+    return HPT_OK;
+  }
   hpt_status admit_pending();
-  hpt_status collect();
+  hpt_status apply_readback(Readback& b);
+  hpt_status finish(Request* r);
+  hpt_status retire_finished();
 };
 
 // Moves queued requests into free slots while the memory budget allows
-// (first fit in arrival order), then runs their primary pass.
+// (first fit in arrival order) and enqueues their primary pass.
 hpt_status hpt_server::admit_pending() {
   std::vector<int> ids;
   std::vector<DevJob> jobs;
@@ -123,7 +197,9 @@ hpt_status hpt_server::admit_pending() {
       ++it;
       continue;
     }
+    HPT_TRACE_BEGIN(alloc_job);
     hpt_status s = engine->alloc_job(r->js, r->want_accum, r->buf);
+    HPT_TRACE_END(alloc_job);
     if (s == HPT_ERR_OUT_OF_MEMORY) {
       engine->free_job(r->buf);
       break;  // retry after something finishes
@@ -132,6 +208,7 @@ hpt_status hpt_server::admit_pending() {
     r->slot = slot;
     r->state = kRunning;
     r->admit_ms = now_ms();
+    r->admit_seq = launched;
     slot_req[slot] = r->id;
     used_bytes += r->footprint;
     ids.push_back(slot);
@@ -144,50 +221,89 @@ hpt_status hpt_server::admit_pending() {
     it = queue.erase(it);
   }
   if (ids.empty()) return HPT_OK;
-  return engine->admit(ids, jobs, rays, order(), nullptr);
+  HPT_TRACE_BEGIN(admit_async);
+  const hpt_status s = engine->admit_async(ids, jobs, rays, order(), nullptr);
+  HPT_TRACE_END(admit_async);
+  return s;
 }
 
-// Reads the slot table; resolves, copies back and releases every request
-// whose paths have all finished.
-hpt_status hpt_server::collect() {
-  hpt_status s = engine->read_state(slot_view, &ctrl_view);
+// Enqueues the resolve and copy-back of a request whose paths all finished.
+hpt_status hpt_server::finish(Request* r) {
+  const hpt_render_params& p = r->js.params;
+  engine->launch_resolve(r->slot, r->js, r->buf);
+  r->rgba_bytes = (size_t)p.sample_x * p.sample_y * 4;
+  void* mem = nullptr;
+  HPT_TRACE_BEGIN(take_pinned);
+  hpt_status s = take_pinned(r->rgba_bytes, &mem);
+  HPT_TRACE_END(take_pinned);
   if (s != HPT_OK) return s;
-  std::vector<Request*> finished;
+  r->rgba = static_cast<uint8_t*>(mem);
+  HPT_CUDA(cudaMemcpyAsync(r->rgba, r->buf.rgba, r->rgba_bytes, cudaMemcpyDeviceToHost,
+                           engine->stream));
+  if (r->want_accum) {
+    r->accum_bytes = (size_t)r->rays * 3 * sizeof(float);
+    s = take_pinned(r->accum_bytes, &mem);
+    if (s != HPT_OK) return s;
+    r->accum = static_cast<float*>(mem);
+    HPT_CUDA(cudaMemcpyAsync(r->accum, r->buf.accum_f, r->accum_bytes, cudaMemcpyDeviceToHost,
+                             engine->stream));
+  }
+  s = take_event(&r->fin_ev);
+  if (s != HPT_OK) return s;
+  HPT_CUDA(cudaEventRecord(r->fin_ev, engine->stream));
+  r->finishing = true;
+  return HPT_OK;
+}
+
+// Applies a completed read-back: progress of the requests admitted before
+// it, and the resolve of those whose paths all finished.
+hpt_status hpt_server::apply_readback(Readback& b) {
+  ctrl_view = *b.ctrl;
+  bool any = false;
   for (size_t k = 0; k < slot_req.size(); ++k) {
     if (!slot_req[k]) continue;
     Request* r = reqs.at(slot_req[k]).get();
-    const DevSlot& S = slot_view[k];
+    if (r->finishing || b.seq <= r->admit_seq) continue;
+    const DevSlot& S = b.slots[k];
     r->paths = S.num_paths;
     r->done_paths = (int64_t)S.done;
     r->queries = r->rays + (int64_t)S.queries;
-    if ((int64_t)S.done >= S.num_paths && S.cursor >= S.num_paths) finished.push_back(r);
-  }
-  if (finished.empty()) return HPT_OK;
-  for (Request* r : finished) {
-    const hpt_render_params& p = r->js.params;
-    engine->launch_resolve(r->slot, r->js, r->buf);
-    r->rgba.resize((size_t)p.sample_x * p.sample_y * 4);
-    HPT_CUDA(cudaMemcpyAsync(r->rgba.data(), r->buf.rgba, r->rgba.size(), cudaMemcpyDeviceToHost,
-                             engine->stream));
-    if (r->want_accum) {
-      r->accum.resize((size_t)r->rays * 3);
-      HPT_CUDA(cudaMemcpyAsync(r->accum.data(), r->buf.accum_f, r->accum.size() * sizeof(float),
-                               cudaMemcpyDeviceToHost, engine->stream));
+    if ((int64_t)S.done >= S.num_paths && S.cursor >= S.num_paths) {
+      hpt_status s = finish(r);
+      if (s != HPT_OK) return s;
+      any = true;
     }
   }
-  HPT_CUDA(cudaStreamSynchronize(engine->stream));
-  const double t = now_ms();
-  for (Request* r : finished) {
+  if (ctrl_view.err.flags & 2u)
+    return fail(HPT_ERR_INVALID_SCENE, "device self-check %d failed (value %lld)",
+                ctrl_view.err.site, (long long)ctrl_view.err.value);
+  if (ctrl_view.err.flags & 1u) return fail(HPT_ERR_TRAVERSAL_LIMIT, "a traversal hit its step cap");
+  return any ? engine->set_order_async(order()) : HPT_OK;
+}
+
+// Marks done the finishing requests whose copy-back has completed and
+// releases their slot and device buffers.
+hpt_status hpt_server::retire_finished() {
+  for (size_t k = 0; k < slot_req.size(); ++k) {
+    if (!slot_req[k]) continue;
+    Request* r = reqs.at(slot_req[k]).get();
+    if (!r->finishing) continue;
+    const cudaError_t e = cudaEventQuery(r->fin_ev);
+    if (e == cudaErrorNotReady) continue;
+    if (e != cudaSuccess) return cuda_fail(e, "copy-back");
+    event_pool.push_back(r->fin_ev);
+    r->fin_ev = nullptr;
+    r->finishing = false;
     engine->free_job(r->buf);
-    slot_req[r->slot] = 0;
+    slot_req[k] = 0;
     used_bytes -= r->footprint;
     r->slot = -1;
     r->state = r->cancel ? kCancelled : kDone;
-    r->done_ms = t;
+    r->done_ms = now_ms();
     finished_ids.push_back(r->id);
     ++completed;
   }
-  return engine->set_order(order());
+  return HPT_OK;
 }
 
 extern "C" {
@@ -197,13 +313,15 @@ hpt_status hpt_server_create(const hpt_server_config* config, hpt_server** out) 
   *out = nullptr;
   if (config->max_jobs < 1 || config->max_jobs > 4096 || config->memory_budget <= 0 ||
       config->capacity < 1024 || config->capacity > (1 << 27) ||
-      config->large_inflight_pct < 0 || config->large_inflight_pct > 100)
+      config->large_inflight_pct < 0 || config->large_inflight_pct > 100 ||
+      config->pipeline_depth < 0 || config->pipeline_depth > kReadbacks - 1)
     return fail(HPT_ERR_INVALID_ARGUMENT, "server config out of range");
   if (config->device < 0 || config->device >= hpt_device_count())
     return fail(HPT_ERR_CUDA, "no CUDA device %d", config->device);
   try {
     std::unique_ptr<hpt_server> s(new hpt_server());
     s->cfg = *config;
+    s->depth = config->pipeline_depth > 0 ? config->pipeline_depth : 1;
     s->t0 = std::chrono::steady_clock::now();
     s->engine.reset(new Engine(config->device));
     s->engine->tuning.capacity = config->capacity;
@@ -221,6 +339,16 @@ hpt_status hpt_server_create(const hpt_server_config* config, hpt_server** out) 
       st = s->engine->set_capped_budget(
           std::max<int64_t>(1024, (int64_t)config->capacity * pct / 100));
       if (st != HPT_OK) return st;
+    }
+    // The admission budget is the per-request device memory the server may
+    // use: map it into the job pool now, so admitting a request never waits
+    // for the driver to map memory.
+    st = s->engine->reserve_pool((size_t)config->memory_budget);
+    if (st != HPT_OK) return st;
+    for (Readback& b : s->rb) {
+      HPT_CUDA(cudaMallocHost(&b.slots, (size_t)config->max_jobs * sizeof(DevSlot)));
+      HPT_CUDA(cudaMallocHost(&b.ctrl, sizeof(DevCtrl)));
+      HPT_CUDA(cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming));
     }
     s->slot_req.assign(config->max_jobs, 0);
     *out = s.release();
@@ -253,6 +381,7 @@ hpt_status hpt_server_submit(hpt_server* server, int32_t scene_slot, const hpt_c
   r->js.scene = &server->scenes[scene_slot]->h.scene;
   r->js.camera = *camera;
   r->js.params = *params;
+  r->want_accum = server->cfg.keep_accum != 0;
   r->rays = (int64_t)params->sample_x * params->supersample_x * params->sample_y *
             params->supersample_y;
   r->footprint = job_footprint(*params, r->want_accum);
@@ -269,22 +398,67 @@ hpt_status hpt_server_submit(hpt_server* server, int32_t scene_slot, const hpt_c
 hpt_status hpt_server_pump(hpt_server* server, int32_t max_iterations) {
   if (!server) return fail(HPT_ERR_INVALID_ARGUMENT, "NULL argument");
   std::lock_guard<std::mutex> lk(server->mu);
-  HPT_CUDA(cudaSetDevice(server->cfg.device));
-  hpt_status s = server->admit_pending();
+  hpt_server& S = *server;
+  HPT_CUDA(cudaSetDevice(S.cfg.device));
+  ++S.pumps;
+  // 1. Completed read-backs, oldest first, and finished copy-backs.
+  auto drain_ready = [&]() -> hpt_status {
+    while (S.rb_pending > 0) {
+      Readback& b = S.rb[S.rb_drain];
+      const cudaError_t e = cudaEventQuery(b.ev);
+      if (e == cudaErrorNotReady) break;
+      if (e != cudaSuccess) return cuda_fail(e, "slot read-back");
+      b.pending = false;
+      S.rb_drain = (S.rb_drain + 1) % kReadbacks;
+      --S.rb_pending;
+      hpt_status s = S.apply_readback(b);
+      if (s != HPT_OK) return s;
+    }
+    return S.retire_finished();
+  };
+  HPT_TRACE_BEGIN(drain);
+  hpt_status s = drain_ready();
+  HPT_TRACE_END(drain);
   if (s != HPT_OK) return s;
-  bool running = false;
-  for (uint64_t id : server->slot_req) running = running || id != 0;
-  if (!running) return HPT_OK;
-  for (int i = 0; i < std::max(1, max_iterations); ++i) server->engine->launch_iteration(nullptr);
+  // 2. Admission.
+  HPT_TRACE_BEGIN(admit);
+  s = S.admit_pending();
+  HPT_TRACE_END(admit);
+  if (s != HPT_OK) return s;
+  HPT_TRACE_BEGIN(launch);
+  // 3. Keep up to `depth` iterations queued, each followed by a read-back.
+  int n = 0;
+  while (n < std::max(1, max_iterations) && S.rb_pending < S.depth && S.running()) {
+    S.engine->launch_iteration(nullptr);
+    ++S.launched;
+    ++n;
+    Readback& b = S.rb[S.rb_fill];
+    b.seq = S.launched;
+    b.pending = true;
+    s = S.engine->read_state_async(b.slots, b.ctrl, b.ev);
+    if (s != HPT_OK) return s;
+    S.rb_fill = (S.rb_fill + 1) % kReadbacks;
+    ++S.rb_pending;
+  }
   HPT_CUDA(cudaGetLastError());
-  ++server->pumps;
-  s = server->collect();
-  if (s != HPT_OK) return s;
-  const DevCtrl& c = server->ctrl_view;
-  if (c.err.flags & 2u)
-    return fail(HPT_ERR_INVALID_SCENE, "device self-check %d failed (value %lld)", c.err.site,
-                (long long)c.err.value);
-  if (c.err.flags & 1u) return fail(HPT_ERR_TRAVERSAL_LIMIT, "a traversal hit its step cap");
+  HPT_TRACE_END(launch);
+  // 4. Nothing new to launch: wait for the oldest read-back (or copy-back)
+  // instead of returning to a caller that would spin.
+  if (n == 0) {
+    HPT_TRACE_BEGIN(wait);
+    if (S.rb_pending > 0) {
+      HPT_CUDA(cudaEventSynchronize(S.rb[S.rb_drain].ev));
+    } else {
+      for (size_t k = 0; k < S.slot_req.size(); ++k)
+        if (S.slot_req[k] && S.reqs.at(S.slot_req[k])->finishing) {
+          HPT_CUDA(cudaEventSynchronize(S.reqs.at(S.slot_req[k])->fin_ev));
+          break;
+        }
+    }
+    HPT_TRACE_END(wait);
+    s = drain_ready();
+    if (s != HPT_OK) return s;
+  }
   return HPT_OK;
 }
 
@@ -307,22 +481,25 @@ hpt_status hpt_server_poll(hpt_server* server, uint64_t request_id, hpt_request_
     info->intersect_queries = r->queries;
   }
   if (r->state == kDone) {
-    if (rgba_out) std::memcpy(rgba_out, r->rgba.data(), r->rgba.size());
-    if (accum_out && r->want_accum)
-      std::memcpy(accum_out, r->accum.data(), r->accum.size() * sizeof(float));
+    if (rgba_out) std::memcpy(rgba_out, r->rgba, r->rgba_bytes);
+    if (accum_out && r->accum) std::memcpy(accum_out, r->accum, r->accum_bytes);
+    server->give_pinned(r->rgba, r->rgba_bytes);
+    server->give_pinned(r->accum, r->accum_bytes);
     server->reqs.erase(request_id);
     return HPT_OK;
   }
   if (r->state == kCancelled || r->state == kFailed) {
     const hpt_status e = r->state == kCancelled ? HPT_ERR_CANCELLED : r->error;
+    server->give_pinned(r->rgba, r->rgba_bytes);
+    server->give_pinned(r->accum, r->accum_bytes);
     server->reqs.erase(request_id);
     return fail(e, "request %llu %s", (unsigned long long)request_id,
                 e == HPT_ERR_CANCELLED ? "was cancelled" : "failed");
   }
   // Running: a progressive preview divides by the samples completed so far
   // (paths finish out of order, so this is the fraction of finished paths).
-  if (r->state == kRunning && server->cfg.progressive && rgba_out && per_sample > 0 &&
-      r->done_paths > 0) {
+  if (r->state == kRunning && !r->finishing && server->cfg.progressive && rgba_out &&
+      per_sample > 0 && r->done_paths > 0) {
     const float samples = (float)((double)r->done_paths / (double)per_sample);
     server->engine->launch_resolve(r->slot, r->js, r->buf, samples);
     HPT_CUDA(cudaMemcpyAsync(rgba_out, r->buf.rgba, (size_t)p.sample_x * p.sample_y * 4,
@@ -388,9 +565,22 @@ void hpt_server_destroy(hpt_server* server) {
     std::lock_guard<std::mutex> lk(server->mu);
     if (server->engine) {
       HPT_SOFT(cudaStreamSynchronize(server->engine->stream));
-      for (auto& kv : server->reqs)
-        if (kv.second->state == kRunning) server->engine->free_job(kv.second->buf);
+      for (auto& kv : server->reqs) {
+        Request* r = kv.second.get();
+        if (r->slot >= 0) server->engine->free_job(r->buf);
+        if (r->fin_ev) HPT_SOFT(cudaEventDestroy(r->fin_ev));
+        if (r->rgba) HPT_SOFT(cudaFreeHost(r->rgba));
+        if (r->accum) HPT_SOFT(cudaFreeHost(r->accum));
+      }
+      HPT_SOFT(cudaStreamSynchronize(server->engine->stream));
     }
+    for (Readback& b : server->rb) {
+      if (b.slots) HPT_SOFT(cudaFreeHost(b.slots));
+      if (b.ctrl) HPT_SOFT(cudaFreeHost(b.ctrl));
+      if (b.ev) HPT_SOFT(cudaEventDestroy(b.ev));
+    }
+    for (auto& kv : server->pinned_pool) HPT_SOFT(cudaFreeHost(kv.second));
+    for (cudaEvent_t e : server->event_pool) HPT_SOFT(cudaEventDestroy(e));
   }
   delete server;
 }

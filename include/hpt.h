@@ -386,14 +386,21 @@ typedef struct hpt_server hpt_server;
 typedef struct hpt_server_config {
   int32_t device;
   int32_t max_jobs;           /* concurrent requests on the GPU           */
-  int64_t memory_budget;      /* bytes of per-request device state        */
+  int64_t memory_budget;      /* bytes of per-request device state; mapped */
+                              /* at creation and kept for the server      */
   int32_t capacity;           /* paths in flight shared by all requests   */
   int32_t progressive;        /* stream partial accumulations             */
   /* Requests with more paths (rays x spp) than `capacity` keep together at
    * most this percentage of `capacity` in flight, so they cannot crowd out
    * the smaller requests admitted after them (0 or 100 = no cap). */
   int32_t large_inflight_pct;
-  int32_t reserved[3];
+  /* Wavefront iterations kept queued on the device ahead of the host's
+   * slot read-backs (0 = 1; at most 7). */
+  int32_t pipeline_depth;
+  /* Keep each request's float accumulator for hpt_server_poll's accum_out
+   * (costs 12 bytes per ray of device memory and copy-back). */
+  int32_t keep_accum;
+  int32_t reserved[1];
 } hpt_server_config;
 
 typedef struct hpt_request_info {
