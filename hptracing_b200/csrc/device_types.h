@@ -2,6 +2,7 @@
 // and the CUDA kernels. Plain structs only: no CUDA headers needed here.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 
 namespace hpt {
@@ -36,6 +37,7 @@ struct DevLeaf {
   int32_t pad;
 };
 static_assert(sizeof(DevLeaf) == 64, "64-byte leaf record");
+static_assert(offsetof(DevLeaf, rope) == 32, "ropes at bytes 32-55 (read as int4 + int2)");
 
 // Triangle record, one per triangle, 48 bytes (3 x 16 B): vertex a,
 // e1 = b - a, e2 = c - a (computed in FP32 exactly as the reference's

@@ -210,12 +210,18 @@ __device__ void schedule(const EngineParams& P) {
 
 // ---------------------------------------------------------------------------
 // Primary pass: raygen + closest hit, lanes refilled from a global counter.
+// Traversal modes of k_primary / k_isect.
+constexpr int kTravLeaf = 0;      // trav_leaf, one leaf per lane per round
+constexpr int kTravStep = 1;      // trav_step, nodes from global memory
+constexpr int kTravStepSmem = 2;  // trav_step with the shared-memory node prefix
+
 // ---------------------------------------------------------------------------
-// kStep: step-at-a-time traversal as in k_isect.
-template <int BS, int MINB, bool kStep>
+// kMode: traversal as in k_isect.
+template <int BS, int MINB, int kMode>
 __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
+  constexpr bool kStep = kMode != kTravLeaf;
   extern __shared__ uint2 snodes[];
-  const int n_smem = stage_nodes(P, snodes);
+  const int n_smem = kMode == kTravStep ? 0 : stage_nodes(P, snodes);
   DevCtrl* c = P.ctrl;
   const int lane = threadIdx.x & 31;
   const int64_t total = P.prim_prefix[P.prim_n];
@@ -261,7 +267,8 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
       if constexpr (kStep) {
         const DevScene& sc = P.jobs[slot].scene;
         for (int u = 0; u < P.trav_steps; ++u)
-          if (trav_step(sc, st, ss, snodes, n_smem, &c->err, cnt)) {
+          if (trav_step<false, kMode == kTravStepSmem>(sc, st, ss, snodes, n_smem, &c->err,
+                                                       cnt)) {
             finished = true;
             break;
           }
@@ -463,13 +470,16 @@ __global__ void __launch_bounds__(BS) k_shade(EngineParams P) {
 // ---------------------------------------------------------------------------
 // Intersect queue -> next shade queue, persistent warps with lane refill.
 // ---------------------------------------------------------------------------
-// kStep: traverse with trav_step, P.trav_steps units per lane between refill
-// checks (lanes move to their next leaf independently); else one leaf per
-// lane per round with trav_leaf.
-template <int BS, int MINB, bool kStep>
+// kMode: kTravStep / kTravStepSmem traverse with trav_step, P.trav_steps
+// calls per lane between refill checks (lanes move to their next leaf
+// independently), reading nodes from global memory only / also from the
+// shared-memory prefix; kTravLeaf: one leaf per lane per round with
+// trav_leaf.
+template <int BS, int MINB, int kMode>
 __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
+  constexpr bool kStep = kMode != kTravLeaf;
   extern __shared__ uint2 snodes[];
-  const int n_smem = stage_nodes(P, snodes);
+  const int n_smem = kMode == kTravStep ? 0 : stage_nodes(P, snodes);
   DevCtrl* c = P.ctrl;
   const int n = c->nR;
   const int out_par = c->parity ^ 1;
@@ -514,7 +524,8 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
       if constexpr (kStep) {
         const DevScene& sc = P.jobs[slot].scene;
         for (int u = 0; u < P.trav_steps; ++u)
-          if (trav_step(sc, st, ss, snodes, n_smem, &c->err, cnt)) {
+          if (trav_step<false, kMode == kTravStepSmem>(sc, st, ss, snodes, n_smem, &c->err,
+                                                       cnt)) {
             finished = true;
             break;
           }
@@ -595,21 +606,31 @@ __global__ void k_ctrl(EngineParams P) {
 // tighter budgets trade spills for resident warps. Chosen by the tuning.
 struct IsectVariant {
   int block, min_blocks;
-  void (*isect)(EngineParams);       // one leaf per round
-  void (*isect_step)(EngineParams);  // step-at-a-time
+  void (*isect)(EngineParams);            // one leaf per round
+  void (*isect_step)(EngineParams);       // step-at-a-time, nodes from global memory
+  void (*isect_step_smem)(EngineParams);  // step-at-a-time, shared-memory node prefix
   void (*primary)(EngineParams);
   void (*primary_step)(EngineParams);
+  void (*primary_step_smem)(EngineParams);
+  // The kernel a launch with these tuning values uses (shared-node prefix
+  // only when smem_nodes > 0).
+  void (*isect_kernel(int trav_steps, int smem_nodes) const)(EngineParams) {
+    return trav_steps <= 0 ? isect : (smem_nodes > 0 ? isect_step_smem : isect_step);
+  }
+  void (*primary_kernel(int trav_steps, int smem_nodes) const)(EngineParams) {
+    return trav_steps <= 0 ? primary : (smem_nodes > 0 ? primary_step_smem : primary_step);
+  }
 };
+#define HPT_ISECT_VARIANT(B, M)                                                       \
+  {B, M, k_isect<B, M, kTravLeaf>, k_isect<B, M, kTravStep>,                          \
+   k_isect<B, M, kTravStepSmem>, k_primary<B, M, kTravLeaf>, k_primary<B, M, kTravStep>, \
+   k_primary<B, M, kTravStepSmem>}
 const IsectVariant kIsectVariants[] = {
-    {128, 5, k_isect<128, 5, false>, k_isect<128, 5, true>, k_primary<128, 5, false>, k_primary<128, 5, true>},
-    {128, 6, k_isect<128, 6, false>, k_isect<128, 6, true>, k_primary<128, 6, false>, k_primary<128, 6, true>},
-    {128, 7, k_isect<128, 7, false>, k_isect<128, 7, true>, k_primary<128, 7, false>, k_primary<128, 7, true>},
-    {128, 8, k_isect<128, 8, false>, k_isect<128, 8, true>, k_primary<128, 8, false>, k_primary<128, 8, true>},
-    {128, 9, k_isect<128, 9, false>, k_isect<128, 9, true>, k_primary<128, 9, false>, k_primary<128, 9, true>},
-    {128, 10, k_isect<128, 10, false>, k_isect<128, 10, true>, k_primary<128, 10, false>, k_primary<128, 10, true>},
-    {256, 2, k_isect<256, 2, false>, k_isect<256, 2, true>, k_primary<256, 2, false>, k_primary<256, 2, true>},
-    {256, 3, k_isect<256, 3, false>, k_isect<256, 3, true>, k_primary<256, 3, false>, k_primary<256, 3, true>},
+    HPT_ISECT_VARIANT(128, 5), HPT_ISECT_VARIANT(128, 6), HPT_ISECT_VARIANT(128, 7),
+    HPT_ISECT_VARIANT(128, 8), HPT_ISECT_VARIANT(128, 9), HPT_ISECT_VARIANT(128, 10),
+    HPT_ISECT_VARIANT(256, 2), HPT_ISECT_VARIANT(256, 3),
 };
+#undef HPT_ISECT_VARIANT
 constexpr int kNumIsectVariants = sizeof(kIsectVariants) / sizeof(kIsectVariants[0]);
 
 __device__ __forceinline__ float ray_value(const unsigned long long* acc, const uint32_t* flags,
@@ -910,6 +931,10 @@ static hpt_status raise_smem_limits(int device) {
     HPT_CUDA(cudaFuncSetAttribute(v.isect, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     HPT_CUDA(cudaFuncSetAttribute(v.isect_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   bytes));
+    HPT_CUDA(cudaFuncSetAttribute(v.primary_step_smem,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    HPT_CUDA(cudaFuncSetAttribute(v.isect_step_smem,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   }
   done[device] = 1;
   return HPT_OK;
@@ -923,7 +948,7 @@ hpt_status Engine::query_occupancy() {
   const size_t smem = (size_t)std::max(0, tuning.smem_nodes) * sizeof(uint2);
   int b = 0;
   HPT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &b, tuning.trav_steps > 0 ? v.isect_step : v.isect, v.block, smem));
+      &b, v.isect_kernel(tuning.trav_steps, tuning.smem_nodes), v.block, smem));
   occ_isect_ = std::max(1, b);
   HPT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<256>, 256, 0));
   occ_shade_ = std::max(1, b);
@@ -1086,10 +1111,7 @@ hpt_status Engine::admit(const std::vector<int>& slot_ids, const std::vector<Dev
                                A_leaf_, R, shared_scene);
   const size_t smem = (size_t)P.smem_nodes * sizeof(uint2);
   const IsectVariant& v = kIsectVariants[isect_variant()];
-  if (P.trav_steps > 0)
-    v.primary_step<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
-  else
-    v.primary<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
+  v.primary_kernel(P.trav_steps, P.smem_nodes)<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
   HPT_CUDA(cudaGetLastError());
   hpt_status s = set_order(order);  // synchronises: the staging is free again
   if (s != HPT_OK) return s;
@@ -1188,10 +1210,7 @@ hpt_status Engine::admit_async(const std::vector<int>& slot_ids, const std::vect
                                A_leaf_, R, shared_scene);
   const size_t smem = (size_t)P.smem_nodes * sizeof(uint2);
   const IsectVariant& v = kIsectVariants[isect_variant()];
-  if (P.trav_steps > 0)
-    v.primary_step<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
-  else
-    v.primary<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
+  v.primary_kernel(P.trav_steps, P.smem_nodes)<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
   k_admit<<<1, 1, 0, stream>>>(P);
   HPT_CUDA(cudaGetLastError());
   return HPT_OK;
@@ -1252,10 +1271,7 @@ void Engine::launch_iteration(const DevScene* shared_scene, cudaEvent_t* ev) {
   if (ev) HPT_SOFT(cudaEventRecord(ev[1], stream));
   const size_t smem = (size_t)P.smem_nodes * sizeof(uint2);
   const IsectVariant& v = kIsectVariants[isect_variant()];
-  if (P.trav_steps > 0)
-    v.isect_step<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
-  else
-    v.isect<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
+  v.isect_kernel(P.trav_steps, P.smem_nodes)<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
   if (ev) HPT_SOFT(cudaEventRecord(ev[2], stream));
   k_ctrl<<<1, 1, 0, stream>>>(P);
 }

@@ -74,7 +74,7 @@ HPT_HD bool mt_test(const Ray& r, const float4 A, const float4 E1,
 // Entries of the per-ray triangle mailbox (a performance knob only: a
 // repeated triangle that misses the mailbox is simply tested again).
 #ifndef HPT_MAILBOX
-#define HPT_MAILBOX 2
+#define HPT_MAILBOX 1
 #endif
 constexpr int kMailbox = HPT_MAILBOX;
 
@@ -313,12 +313,16 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, const uint2* smem,
 // instead of waiting for the lane with the deepest descent and then for the
 // one with the longest triangle list; results are identical to trav_leaf's
 // (same tests in the same order, same termination).
+// Each call runs exactly one unit: letting a lane fall through from set-up
+// to its first test, or from its last test to the exit, in the same call
+// needs fewer calls per ray but measured slower (more registers live across
+// the three blocks).
 struct StepState {
   int32_t phase;      // kStepDescend / kStepTest
   int32_t k, end;     // next position in leaf_refs / end of the leaf's list
   int32_t leaf;       // leaf record of the current leaf
   int32_t leaf_node;  // its node index (reported as best_node)
-  int32_t face;       // exit face, -1 when the leaf has none
+  int32_t rope;       // node behind the exit face, -1 when there is none
   int32_t pierced;    // reference box test of the leaf: -1 not evaluated yet
   float t_exit;
 };
@@ -329,20 +333,22 @@ HPT_HD void step_init(StepState& ss) {
   ss.phase = kStepDescend;
   ss.k = ss.end = 0;
   ss.leaf = ss.leaf_node = 0;
-  ss.face = -1;
+  ss.rope = -1;
   ss.pierced = -1;
   ss.t_exit = 0.f;
 }
 
 // Returns true when the ray is finished.
-template <bool kUV = false>
+// kSmem: nodes below n_smem are read from the shared-memory prefix (false:
+// every node from global memory, and smem / n_smem are ignored).
+template <bool kUV = false, bool kSmem = true>
 HPT_HD bool trav_step(const DevScene& s, TravState& st, StepState& ss, const uint2* smem,
                       int n_smem, DevErr* err, TravCount& cnt) {
   if (st.node < 0) return true;
   const Ray& r = st.ray;
   if (ss.phase == kStepDescend) {
     HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
-    const uint2 nd = fetch_node(s, smem, n_smem, st.node);
+    const uint2 nd = fetch_node(s, smem, kSmem ? n_smem : 0, st.node);
     if ((nd.x >> 30) != kLeafKind) {
       // One descent step; the entry point p = o + t_entry * d on the split
       // axis (kernel.cl:291 style, no FMA), as trav_leaf computes it.
@@ -368,7 +374,11 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, StepState& ss, const uin
                { st.node = -1; return true; });
     const int leaf = (int)(nd.x & kIndexMask);
     const float4* L = reinterpret_cast<const float4*>(s.leaves + leaf);
+    // The six ropes are read with the box (independent loads) so that the
+    // exit needs no dependent load of its own.
     const float4 L0 = ldg(L), L1 = ldg(L + 1);
+    const int4 R03 = ldg(reinterpret_cast<const int4*>(L + 2));
+    const int2 R45 = ldg(reinterpret_cast<const int2*>(L + 3));
     float t_exit = as_float(0x7f800000);
     int face = -1;
     {
@@ -399,7 +409,8 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, StepState& ss, const uin
     ss.end = begin + count;
     ss.leaf = leaf;
     ss.leaf_node = st.node;
-    ss.face = face;
+    ss.rope = face == 0 ? R03.x : face == 1 ? R03.y : face == 2 ? R03.z
+            : face == 3 ? R03.w : face == 4 ? R45.x : face == 5 ? R45.y : -1;
     ss.t_exit = t_exit;
     ss.pierced = -1;
     ss.phase = kStepTest;
@@ -460,9 +471,10 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, StepState& ss, const uin
     return false;
   }
   // Leaf exit: stop once the rest of the ray starts beyond the best hit
-  // (+ slack), else follow the exit rope.
+  // (+ slack), else follow the exit rope. A leaf without an exit face has
+  // t_exit = +inf and stops here.
   ss.phase = kStepDescend;
-  if (ss.face < 0 || !(ss.t_exit < st.t_end)) {
+  if (!(ss.t_exit < st.t_end)) {
     st.node = -1;
     return true;
   }
@@ -471,8 +483,7 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, StepState& ss, const uin
     st.node = -1;
     return true;
   }
-  const int rope =
-      ldg(reinterpret_cast<const int*>(s.leaves + ss.leaf) + 8 + ss.face);
+  const int rope = ss.rope;
   if (rope < 0 || st.steps > s.max_steps) {
     if (rope >= 0) hpt_atomic_or(&err->flags, 1u);
     st.node = -1;
