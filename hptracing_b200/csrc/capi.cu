@@ -69,10 +69,11 @@ __global__ void k_stage_intersect(const DevScene* s, int n, const float* o, cons
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   TravState st;
+  TravCold tc;
   trav_init(*s, Ray{mk(o[3 * i], o[3 * i + 1], o[3 * i + 2]), mk(d[3 * i], d[3 * i + 1], d[3 * i + 2])},
-            st);
-  TravCount cnt;
-  while (!trav_leaf<true>(*s, st, nullptr, 0, err, cnt)) {
+            st, tc);
+  TravCount cnt{};
+  while (!trav_leaf<true>(*s, st, tc, nullptr, 0, err, cnt)) {
   }
   tri[i] = st.best.tri;
   t[i] = st.best.rec >= 0 ? st.best.t : 0.f;

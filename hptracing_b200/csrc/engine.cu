@@ -129,6 +129,14 @@ __device__ __forceinline__ void count_queries(DevSlot* slots, bool alive, int sl
     atomicAdd(&slots[slot].queries, (unsigned long long)__popc(same & m));
 }
 
+// A lane's work counters in shared memory (five words: an odd stride, so
+// the lanes of a warp hit distinct banks); they are touched once per
+// traversal unit and would otherwise hold four registers.
+struct CountSlot {
+  TravCount c;
+  uint32_t pad;
+};
+
 // Warp-level reduction of the per-lane query and work counters.
 __device__ __forceinline__ void flush_counts(DevCtrl* c, unsigned long long q, TravCount lane) {
   unsigned long long nodes = lane.nodes, leaves = lane.leaves, tris = lane.tris,
@@ -227,11 +235,14 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
   const int64_t total = P.prim_prefix[P.prim_n];
   bool active = false;
   TravState st;
-  StepState ss;
+  __shared__ TravCold cold_sh[BS];
+  __shared__ CountSlot count_sh[BS];
+  TravCold& tc = cold_sh[threadIdx.x];
+  TravCount& cnt = count_sh[threadIdx.x].c;
+  cnt = TravCount{};
   int slot = 0;
   int64_t ray = 0;
   uint32_t queries = 0;  // this lane's queries in this launch
-  TravCount cnt;
   while (true) {
     const unsigned idle = __ballot_sync(kFull, !active);
     if (__popc(idle) >= P.refill) {
@@ -253,8 +264,7 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
             const int x = (int)(ray % J.nx), y = (int)(ray / J.nx);
             const f3 d = J.pano ? pano_dir(x, y, J.vr_x_shift, J.ny)
                                 : pinhole_dir(J.top, J.right, J.width, J.height, x, y, J.nx, J.ny);
-            trav_init(J.scene, Ray{mk(J.view_p[0], J.view_p[1], J.view_p[2]), d}, st);
-            if (kStep) step_init(ss);
+            trav_init(J.scene, Ray{mk(J.view_p[0], J.view_p[1], J.view_p[2]), d}, st, tc);
             active = true;
             ++queries;
           }
@@ -267,13 +277,13 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
       if constexpr (kStep) {
         const DevScene& sc = P.jobs[slot].scene;
         for (int u = 0; u < P.trav_steps; ++u)
-          if (trav_step<false, kMode == kTravStepSmem>(sc, st, ss, snodes, n_smem, &c->err,
+          if (trav_step<false, kMode == kTravStepSmem>(sc, st, tc, snodes, n_smem, &c->err,
                                                        cnt)) {
             finished = true;
             break;
           }
       } else {
-        finished = trav_leaf(P.jobs[slot].scene, st, snodes, n_smem, &c->err, cnt);
+        finished = trav_leaf(P.jobs[slot].scene, st, tc, snodes, n_smem, &c->err, cnt);
       }
     }
     if (finished) {
@@ -285,7 +295,7 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
           float4* dst = reinterpret_cast<float4*>(J.prim) + 2 * (size_t)k;
           dst[0] = make_float4(st.ray.d.x, st.ray.d.y, st.ray.d.z, __int_as_float((int)ray));
           dst[1] = make_float4(__int_as_float(st.best.tri), st.best.t,
-                               __int_as_float(st.best_node), 0.f);
+                               __int_as_float(tc.best_node), 0.f);
         }
       } else {
         // kernel.cl:193-206: the first pass assigns background * strength *
@@ -486,11 +496,14 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
   const int lane = threadIdx.x & 31;
   bool active = false;
   TravState st;
-  StepState ss;
+  __shared__ TravCold cold_sh[BS];
+  __shared__ CountSlot count_sh[BS];
+  TravCold& tc = cold_sh[threadIdx.x];
+  TravCount& cnt = count_sh[threadIdx.x].c;
+  cnt = TravCount{};
   int item = 0;   // index in the intersect queue; the payload is reloaded at the end
   int slot = 0;
   uint32_t queries = 0;  // this lane's queries in this launch
-  TravCount cnt;
   while (true) {
     const unsigned idle = __ballot_sync(kFull, !active);
     if (__popc(idle) >= P.refill) {
@@ -509,8 +522,7 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
             HPT_DCHECK(&c->err, slot >= 0 && slot < P.num_slots, 222, slot, ok = false);
             if (ok) {
               trav_init(P.jobs[slot].scene, Ray{mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z)}, st,
-                        __float_as_int(P.R_r[i].w));
-              if (kStep) step_init(ss);
+                        tc, __float_as_int(P.R_r[i].w));
               active = true;
               ++queries;
             }
@@ -524,13 +536,13 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
       if constexpr (kStep) {
         const DevScene& sc = P.jobs[slot].scene;
         for (int u = 0; u < P.trav_steps; ++u)
-          if (trav_step<false, kMode == kTravStepSmem>(sc, st, ss, snodes, n_smem, &c->err,
+          if (trav_step<false, kMode == kTravStepSmem>(sc, st, tc, snodes, n_smem, &c->err,
                                                        cnt)) {
             finished = true;
             break;
           }
       } else {
-        finished = trav_leaf(P.jobs[slot].scene, st, snodes, n_smem, &c->err, cnt);
+        finished = trav_leaf(P.jobs[slot].scene, st, tc, snodes, n_smem, &c->err, cnt);
       }
     }
     const bool hit = finished && st.best.rec >= 0;
@@ -551,7 +563,7 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
           P.A_s[out_par][pos] = P.R_s[item];
           P.A_r[out_par][pos] = make_float4(r4.x, r4.y, r4.z, st.best.t);
           P.A_tri[out_par][pos] = st.best.tri;
-          P.A_leaf[out_par][pos] = st.best_node;
+          P.A_leaf[out_par][pos] = tc.best_node;
         }
       }
     }
@@ -713,12 +725,14 @@ void cuda_soft_fail(cudaError_t e, const char* what) {
 hpt_tuning default_tuning() {
   hpt_tuning t;
   memset(&t, 0, sizeof t);
-  // From the tuning sweep on the 61k-triangle spheres frame (512x512, 64 spp):
-  // step-at-a-time traversal, 24 units per refill check, 8 blocks of 128 per
-  // SM (64 registers), no shared-node prefix.
+  // From the tuning sweeps on the 61k-triangle spheres frame (512x512,
+  // 64 spp) and the 2.4M-triangle terrain frame: step-at-a-time traversal,
+  // 24 units per refill check, 10 blocks of 128 per SM (48 registers; the
+  // per-leaf state and counters live in shared memory), no shared-node
+  // prefix.
   t.capacity = 1 << 22;
   t.isect_block = 128;
-  t.isect_min_blocks = 8;
+  t.isect_min_blocks = 10;
   t.shade_block = 256;
   t.refill_chunk = 4;
   t.smem_nodes = 0;

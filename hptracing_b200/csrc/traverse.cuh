@@ -78,42 +78,73 @@ HPT_HD bool mt_test(const Ray& r, const float4 A, const float4 E1,
 #endif
 constexpr int kMailbox = HPT_MAILBOX;
 
-// Traversal state of one ray; lives in registers so a lane can be
-// refilled with a new ray between leaves.
+// Phases of the step-at-a-time walk (trav_step).
+constexpr int32_t kStepDescend = 0;
+constexpr int32_t kStepTest = 1;
+
+// Traversal state of one ray that most units touch; lives in registers so
+// a lane can be refilled with a new ray between leaves.
 struct TravState {
   Ray ray;
-  f3 inv_d;              // 1 / d (exit distances only; the filter divides)
-  float t_entry, t_end;  // current entry distance, scene exit distance
-  float slack;           // world-space rounding slack in t units
+  float t_entry;         // current entry distance
   int32_t node;          // node to descend from, -1 = finished
   int32_t steps;
-  int32_t best_node;     // leaf node where the best hit was found
   Hit best;
   // The last kMailbox triangles tested and their Moller-Trumbore t (-1 =
   // miss): the reference tree repeats a triangle in every leaf it straddles.
   int32_t mb_id[kMailbox];
   float mb_t[kMailbox];
+  // trav_step only: kStepDescend / kStepTest, and in a leaf the next
+  // position in leaf_refs and the end of its list.
+  int32_t phase;
+  int32_t k, end;
 };
+
+// The rest of a ray's traversal state: written when the query starts or a
+// leaf is set up, read at a leaf's exit or when a candidate would win -
+// at most a few times per leaf. The kernels keep it in shared memory
+// (eleven words per lane: an odd stride, free of bank conflicts) so that
+// the registers go to the state every unit touches.
+struct TravCold {
+  f3 inv_d;           // 1 / d (exit distances only; the filter divides)
+  float t_end;        // scene exit distance
+  float slack;        // world-space rounding slack in t units
+  int32_t best_node;  // leaf node where the best hit was found
+  // trav_step's current leaf:
+  int32_t leaf;       // leaf record
+  int32_t leaf_node;  // its node index (reported as best_node)
+  int32_t rope;       // node behind the exit face, -1 when there is none
+  int32_t pierced;    // reference box test of the leaf: -1 not evaluated yet
+  float t_exit;
+};
+static_assert(sizeof(TravCold) == 44, "odd word stride in shared memory");
 
 // Work counters of one lane over one kernel launch (summed per warp in 64
 // bits when the launch ends; they feed statistics only).
+// (Plain data: declare with `TravCount cnt{}` to start from zero.)
 struct TravCount {
-  uint32_t nodes = 0, leaves = 0, tris = 0, repeats = 0;
+  uint32_t nodes, leaves, tris, repeats;
 };
 
 // Starts a query. start_node (>= 0) names a leaf node the origin is
 // expected to lie in (the leaf of the previous hit): if its box contains the
 // origin the walk starts there instead of descending from the root.
-HPT_HD void trav_init(const DevScene& s, const Ray& r, TravState& st,
-                                          int start_node = -1) {
+HPT_HD void trav_init(const DevScene& s, const Ray& r, TravState& st, TravCold& tc,
+                      int start_node = -1) {
   st.ray = r;
   st.best.rec = -1;
   st.best.tri = -1;
   st.best.t = 0.f;
   st.best.u = st.best.v = 0.f;
-  st.best_node = -1;
+  tc.best_node = -1;
+  tc.leaf = tc.leaf_node = 0;
+  tc.rope = -1;
+  tc.pierced = -1;
+  tc.t_exit = 0.f;
   st.steps = 0;
   st.node = -1;
+  st.phase = kStepDescend;
+  st.k = st.end = 0;
 #pragma unroll
   for (int k = 0; k < kMailbox; ++k) {
     st.mb_id[k] = -1;
@@ -137,10 +168,10 @@ HPT_HD void trav_init(const DevScene& s, const Ray& r, TravState& st,
     }
   }
   if (!(dmax > 0.f) || !(t0 <= t1)) return;
-  st.inv_d = mk(rn_rcp(r.d.x), rn_rcp(r.d.y), rn_rcp(r.d.z));
+  tc.inv_d = mk(rn_rcp(r.d.x), rn_rcp(r.d.y), rn_rcp(r.d.z));
   st.t_entry = t0;
-  st.t_end = t1;
-  st.slack = rn_div(s.scene_eps, dmax);
+  tc.t_end = t1;
+  tc.slack = rn_div(s.scene_eps, dmax);
   st.node = 0;
   if (start_node > 0 && start_node < s.num_nodes) {
     const uint2 nd = ldg(reinterpret_cast<const uint2*>(s.nodes) + start_node);
@@ -171,8 +202,8 @@ constexpr uint32_t kDeadLeafMeta = 0xFFFFFFFFu;
 // Returns true when the ray is finished.
 // kUV: also report the winning test's Moller-Trumbore u, v (stage entry).
 template <bool kUV = false>
-HPT_HD bool trav_leaf(const DevScene& s, TravState& st, const uint2* smem,
-                                          int n_smem, DevErr* err, TravCount& cnt) {
+HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint2* smem,
+                      int n_smem, DevErr* err, TravCount& cnt) {
   if (st.node < 0) return true;
   HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
   const Ray& r = st.ray;
@@ -211,7 +242,7 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, const uint2* smem,
   {
     const float d[3] = {r.d.x, r.d.y, r.d.z};
     const float o[3] = {r.o.x, r.o.y, r.o.z};
-    const float iv[3] = {st.inv_d.x, st.inv_d.y, st.inv_d.z};
+    const float iv[3] = {tc.inv_d.x, tc.inv_d.y, tc.inv_d.z};
     const float lo[3] = {L0.x, L0.y, L0.z};
     const float hi[3] = {L1.x, L1.y, L1.z};
 #pragma unroll
@@ -280,16 +311,16 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, const uint2* smem,
             st.best.u = u;
             st.best.v = v;
           }
-          st.best_node = node;
+          tc.best_node = node;
         }
       }
     }
   }
   st.steps += 1 + count;
   // Stop once the rest of the ray starts beyond the best hit (+ slack).
-  if (face < 0 || !(t_exit < st.t_end)) { st.node = -1; return true; }
+  if (face < 0 || !(t_exit < tc.t_end)) { st.node = -1; return true; }
   if (st.best.rec >= 0 &&
-      t_exit > rn_add(st.best.t, rn_add(rn_mul(st.best.t, 1e-4f), st.slack))) {
+      t_exit > rn_add(st.best.t, rn_add(rn_mul(st.best.t, 1e-4f), tc.slack))) {
     st.node = -1;
     return true;
   }
@@ -317,36 +348,16 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, const uint2* smem,
 // to its first test, or from its last test to the exit, in the same call
 // needs fewer calls per ray but measured slower (more registers live across
 // the three blocks).
-struct StepState {
-  int32_t phase;      // kStepDescend / kStepTest
-  int32_t k, end;     // next position in leaf_refs / end of the leaf's list
-  int32_t leaf;       // leaf record of the current leaf
-  int32_t leaf_node;  // its node index (reported as best_node)
-  int32_t rope;       // node behind the exit face, -1 when there is none
-  int32_t pierced;    // reference box test of the leaf: -1 not evaluated yet
-  float t_exit;
-};
-constexpr int32_t kStepDescend = 0;
-constexpr int32_t kStepTest = 1;
-
-HPT_HD void step_init(StepState& ss) {
-  ss.phase = kStepDescend;
-  ss.k = ss.end = 0;
-  ss.leaf = ss.leaf_node = 0;
-  ss.rope = -1;
-  ss.pierced = -1;
-  ss.t_exit = 0.f;
-}
 
 // Returns true when the ray is finished.
 // kSmem: nodes below n_smem are read from the shared-memory prefix (false:
 // every node from global memory, and smem / n_smem are ignored).
 template <bool kUV = false, bool kSmem = true>
-HPT_HD bool trav_step(const DevScene& s, TravState& st, StepState& ss, const uint2* smem,
+HPT_HD bool trav_step(const DevScene& s, TravState& st, TravCold& tc, const uint2* smem,
                       int n_smem, DevErr* err, TravCount& cnt) {
   if (st.node < 0) return true;
   const Ray& r = st.ray;
-  if (ss.phase == kStepDescend) {
+  if (st.phase == kStepDescend) {
     HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
     const uint2 nd = fetch_node(s, smem, kSmem ? n_smem : 0, st.node);
     if ((nd.x >> 30) != kLeafKind) {
@@ -384,7 +395,7 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, StepState& ss, const uin
     {
       const float d[3] = {r.d.x, r.d.y, r.d.z};
       const float o[3] = {r.o.x, r.o.y, r.o.z};
-      const float iv[3] = {st.inv_d.x, st.inv_d.y, st.inv_d.z};
+      const float iv[3] = {tc.inv_d.x, tc.inv_d.y, tc.inv_d.z};
       const float lo[3] = {L0.x, L0.y, L0.z};
       const float hi[3] = {L1.x, L1.y, L1.z};
 #pragma unroll
@@ -405,20 +416,20 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, StepState& ss, const uin
     // trav_leaf adds the leaf's cost when it leaves it; every comparison with
     // max_steps comes later in both orders, so adding it here is equivalent.
     st.steps += 1 + count;
-    ss.k = begin;
-    ss.end = begin + count;
-    ss.leaf = leaf;
-    ss.leaf_node = st.node;
-    ss.rope = face == 0 ? R03.x : face == 1 ? R03.y : face == 2 ? R03.z
+    st.k = begin;
+    st.end = begin + count;
+    tc.leaf = leaf;
+    tc.leaf_node = st.node;
+    tc.rope = face == 0 ? R03.x : face == 1 ? R03.y : face == 2 ? R03.z
             : face == 3 ? R03.w : face == 4 ? R45.x : face == 5 ? R45.y : -1;
-    ss.t_exit = t_exit;
-    ss.pierced = -1;
-    ss.phase = kStepTest;
+    tc.t_exit = t_exit;
+    tc.pierced = -1;
+    st.phase = kStepTest;
     return false;
   }
-  if (ss.k < ss.end) {
+  if (st.k < st.end) {
     // One triangle test (the body of trav_leaf's triangle loop).
-    const int j = ss.k++;
+    const int j = st.k++;
     const int id = ldg(s.leaf_refs + j);
     HPT_DCHECK(err, id >= 0 && id < s.num_triangles, 104, id, return false);
     const float4* recs = reinterpret_cast<const float4*>(s.tris);
@@ -448,11 +459,11 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, StepState& ss, const uin
       st.mb_t[0] = t;
     }
     if (t > 0.f && (st.best.rec < 0 || t < st.best.t || (t == st.best.t && j < st.best.rec))) {
-      if (ss.pierced < 0) {
-        const float4* L = reinterpret_cast<const float4*>(s.leaves + ss.leaf);
-        ss.pierced = ref_box_test(r, ldg(L), ldg(L + 1)) ? 1 : 0;
+      if (tc.pierced < 0) {
+        const float4* L = reinterpret_cast<const float4*>(s.leaves + tc.leaf);
+        tc.pierced = ref_box_test(r, ldg(L), ldg(L + 1)) ? 1 : 0;
       }
-      if (ss.pierced) {
+      if (tc.pierced) {
         if (kUV && !tested) {  // a repeat that now wins: recover its u, v
           const float4* rec = recs + 3 * (size_t)id;
           float t2;
@@ -465,7 +476,7 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, StepState& ss, const uin
           st.best.u = u;
           st.best.v = v;
         }
-        st.best_node = ss.leaf_node;
+        tc.best_node = tc.leaf_node;
       }
     }
     return false;
@@ -473,17 +484,17 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, StepState& ss, const uin
   // Leaf exit: stop once the rest of the ray starts beyond the best hit
   // (+ slack), else follow the exit rope. A leaf without an exit face has
   // t_exit = +inf and stops here.
-  ss.phase = kStepDescend;
-  if (!(ss.t_exit < st.t_end)) {
+  st.phase = kStepDescend;
+  if (!(tc.t_exit < tc.t_end)) {
     st.node = -1;
     return true;
   }
   if (st.best.rec >= 0 &&
-      ss.t_exit > rn_add(st.best.t, rn_add(rn_mul(st.best.t, 1e-4f), st.slack))) {
+      tc.t_exit > rn_add(st.best.t, rn_add(rn_mul(st.best.t, 1e-4f), tc.slack))) {
     st.node = -1;
     return true;
   }
-  const int rope = ss.rope;
+  const int rope = tc.rope;
   if (rope < 0 || st.steps > s.max_steps) {
     if (rope >= 0) hpt_atomic_or(&err->flags, 1u);
     st.node = -1;
@@ -491,7 +502,7 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, StepState& ss, const uin
   }
   HPT_DCHECK(err, rope < s.num_nodes, 105, rope, { st.node = -1; return true; });
   st.node = rope;
-  st.t_entry = fmaxf(st.t_entry, ss.t_exit);
+  st.t_entry = fmaxf(st.t_entry, tc.t_exit);
   return false;
 }
 

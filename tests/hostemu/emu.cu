@@ -111,18 +111,19 @@ void emu_intersect(void* h, int n, const float* o, const float* d, const int* hi
   }
   DevErr de;
   memset(&de, 0, sizeof de);
-  TravCount cnt;
+  TravCount cnt{};
   for (int i = 0; i < n; ++i) {
     TravState st;
+    TravCold tc;
     trav_init(s, Ray{mk(o[3 * i], o[3 * i + 1], o[3 * i + 2]), mk(d[3 * i], d[3 * i + 1], d[3 * i + 2])},
-              st, hints ? hints[i] : -1);
-    while (!trav_leaf<true>(s, st, smem.data(), (int)smem.size(), &de, cnt)) {
+              st, tc, hints ? hints[i] : -1);
+    while (!trav_leaf<true>(s, st, tc, smem.data(), (int)smem.size(), &de, cnt)) {
     }
     tri[i] = st.best.tri;
     t[i] = st.best.rec >= 0 ? st.best.t : 0.f;
     u[i] = st.best.rec >= 0 ? st.best.u : 0.f;
     v[i] = st.best.rec >= 0 ? st.best.v : 0.f;
-    if (best_node) best_node[i] = st.best_node;
+    if (best_node) best_node[i] = tc.best_node;
   }
   counters[0] = (long long)cnt.nodes;
   counters[1] = (long long)cnt.leaves;
@@ -146,20 +147,19 @@ void emu_intersect_step(void* h, int n, const float* o, const float* d, const in
   }
   DevErr de;
   memset(&de, 0, sizeof de);
-  TravCount cnt;
+  TravCount cnt{};
   for (int i = 0; i < n; ++i) {
     TravState st;
-    StepState ss;
-    step_init(ss);
+    TravCold tc;
     trav_init(s, Ray{mk(o[3 * i], o[3 * i + 1], o[3 * i + 2]), mk(d[3 * i], d[3 * i + 1], d[3 * i + 2])},
-              st, hints ? hints[i] : -1);
-    while (!trav_step<true>(s, st, ss, smem.data(), (int)smem.size(), &de, cnt)) {
+              st, tc, hints ? hints[i] : -1);
+    while (!trav_step<true>(s, st, tc, smem.data(), (int)smem.size(), &de, cnt)) {
     }
     tri[i] = st.best.tri;
     t[i] = st.best.rec >= 0 ? st.best.t : 0.f;
     u[i] = st.best.rec >= 0 ? st.best.u : 0.f;
     v[i] = st.best.rec >= 0 ? st.best.v : 0.f;
-    if (best_node) best_node[i] = st.best_node;
+    if (best_node) best_node[i] = tc.best_node;
   }
   counters[0] = (long long)cnt.nodes;
   counters[1] = (long long)cnt.leaves;
