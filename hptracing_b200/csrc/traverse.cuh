@@ -344,10 +344,12 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint
 // instead of waiting for the lane with the deepest descent and then for the
 // one with the longest triangle list; results are identical to trav_leaf's
 // (same tests in the same order, same termination).
-// Each call runs exactly one unit: letting a lane fall through from set-up
-// to its first test, or from its last test to the exit, in the same call
-// needs fewer calls per ray but measured slower (more registers live across
-// the three blocks).
+// A call runs one unit, except that a leaf's last triangle test falls
+// through to the leaf's exit in the same call: the exit needs no load of
+// its own (the ropes are read at set-up), so this saves a call per leaf for
+// a few instructions. Falling through from set-up to the first test as
+// well measured slower (the set-up's loads and the test's loads then
+// chain within one call).
 
 // Returns true when the ray is finished.
 // kSmem: nodes below n_smem are read from the shared-memory prefix (false:
@@ -479,7 +481,8 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, TravCold& tc, const uint
         tc.best_node = tc.leaf_node;
       }
     }
-    return false;
+    if (st.k < st.end) return false;
+    // The leaf's last test falls through to its exit.
   }
   // Leaf exit: stop once the rest of the ray starts beyond the best hit
   // (+ slack), else follow the exit rope. A leaf without an exit face has
