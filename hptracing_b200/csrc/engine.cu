@@ -70,6 +70,13 @@ struct EngineParams {
   int refill;
   int trav_steps;       // > 0: step-at-a-time traversal, units per round
   const DevNode* shared_nodes;
+  // When every job of the launch renders the same scene (a frame, or a
+  // batch over one scene): a copy of its DevScene in the kernel's parameter
+  // space. The step loop then reads the scene's pointers and sizes as
+  // constant operands instead of loading them from the job table on every
+  // traversal unit (one dependent load less per unit).
+  int uniform_scene;
+  DevScene uscene;
 };
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -275,13 +282,22 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
     bool finished = false;
     if (active) {
       if constexpr (kStep) {
-        const DevScene& sc = P.jobs[slot].scene;
-        for (int u = 0; u < P.trav_steps; ++u)
-          if (trav_step<false, kMode == kTravStepSmem>(sc, st, tc, snodes, n_smem, &c->err,
-                                                       cnt)) {
-            finished = true;
-            break;
-          }
+        if (P.uniform_scene) {
+          for (int u = 0; u < P.trav_steps; ++u)
+            if (trav_step<false, kMode == kTravStepSmem>(P.uscene, st, tc, snodes, n_smem,
+                                                         &c->err, cnt)) {
+              finished = true;
+              break;
+            }
+        } else {
+          const DevScene& sc = P.jobs[slot].scene;
+          for (int u = 0; u < P.trav_steps; ++u)
+            if (trav_step<false, kMode == kTravStepSmem>(sc, st, tc, snodes, n_smem, &c->err,
+                                                         cnt)) {
+              finished = true;
+              break;
+            }
+        }
       } else {
         finished = trav_leaf(P.jobs[slot].scene, st, tc, snodes, n_smem, &c->err, cnt);
       }
@@ -534,13 +550,22 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
     bool finished = false;
     if (active) {
       if constexpr (kStep) {
-        const DevScene& sc = P.jobs[slot].scene;
-        for (int u = 0; u < P.trav_steps; ++u)
-          if (trav_step<false, kMode == kTravStepSmem>(sc, st, tc, snodes, n_smem, &c->err,
-                                                       cnt)) {
-            finished = true;
-            break;
-          }
+        if (P.uniform_scene) {
+          for (int u = 0; u < P.trav_steps; ++u)
+            if (trav_step<false, kMode == kTravStepSmem>(P.uscene, st, tc, snodes, n_smem,
+                                                         &c->err, cnt)) {
+              finished = true;
+              break;
+            }
+        } else {
+          const DevScene& sc = P.jobs[slot].scene;
+          for (int u = 0; u < P.trav_steps; ++u)
+            if (trav_step<false, kMode == kTravStepSmem>(sc, st, tc, snodes, n_smem, &c->err,
+                                                         cnt)) {
+              finished = true;
+              break;
+            }
+        }
       } else {
         finished = trav_leaf(P.jobs[slot].scene, st, tc, snodes, n_smem, &c->err, cnt);
       }
@@ -1063,6 +1088,10 @@ static EngineParams make_params(const Engine& e, DevCtrl* ctrl, DevJob* jobs, De
   P.capacity = capacity;
   P.refill = std::max(1, std::min(32, e.tuning.refill_chunk));
   P.trav_steps = std::max(0, e.tuning.trav_steps);
+  if (shared) {
+    P.uniform_scene = 1;
+    P.uscene = *shared;
+  }
   if (shared && e.tuning.smem_nodes > 0) {
     P.smem_nodes = std::min(e.tuning.smem_nodes, shared->num_nodes);
     P.shared_nodes = shared->nodes;
