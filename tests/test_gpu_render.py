@@ -94,6 +94,9 @@ def test_render_reference_estimator_3sigma(room):
 
 
 def test_render_deterministic_and_batch_equal(room, spheres):
+    """Renders repeat bit for bit, and a batch over two scenes (traversal
+    reading each job's scene from the job table) gives the bits of the
+    one-scene renders (scene read from the kernel parameters)."""
     _, g0, _ = room
     _, g1, _ = spheres
     a1 = _render(g0, S.ROOM_CAM, 40, 30, 2, 3, 5, seed=4)[1]
