@@ -1269,8 +1269,14 @@ hpt_status Engine::read_state_async(DevSlot* slots, DevCtrl* ctrl, cudaEvent_t e
 }
 
 hpt_status Engine::ensure_graph(const DevScene* shared_scene, int iterations) {
-  const void* key_nodes = shared_scene ? (const void*)shared_scene->nodes : nullptr;
-  if (graph_exec_ && graph_nodes_ == key_nodes && graph_capacity_ == capacity_ &&
+  // The key covers the whole shared scene, not just its node array: a scene
+  // freed and replaced by one whose nodes land at the same address must not
+  // reuse a graph that holds the old scene's other pointers.
+  const bool shared = shared_scene != nullptr;
+  const bool same_scene =
+      graph_shared_ == shared &&
+      (!shared || memcmp(&graph_scene_, shared_scene, sizeof(DevScene)) == 0);
+  if (graph_exec_ && same_scene && graph_capacity_ == capacity_ &&
       graph_slots_ == slots_ && graph_iters_ == iterations && graph_tuning_ == isect_variant() &&
       graph_smem_ == tuning.smem_nodes && graph_refill_ == tuning.refill_chunk &&
       graph_steps_ == tuning.trav_steps)
@@ -1292,7 +1298,8 @@ hpt_status Engine::ensure_graph(const DevScene* shared_scene, int iterations) {
   const cudaError_t inst = cudaGraphInstantiate(&graph_exec_, g, 0);
   HPT_SOFT(cudaGraphDestroy(g));
   HPT_CUDA(inst);
-  graph_nodes_ = key_nodes;
+  graph_shared_ = shared;
+  if (shared) graph_scene_ = *shared_scene;
   graph_capacity_ = capacity_;
   graph_slots_ = slots_;
   graph_iters_ = iterations;

@@ -152,7 +152,10 @@ class Engine {
   hpt_status next_staging(StagingSet** out);
   hpt_status upload_order(const std::vector<int>& order, StagingSet& st);
   cudaGraphExec_t graph_exec_ = nullptr;
-  const void* graph_nodes_ = nullptr;
+  // The one scene the captured iterations were launched with (its pointers
+  // and sizes are baked into the graph's kernel parameters), if any.
+  bool graph_shared_ = false;
+  DevScene graph_scene_{};
   int graph_capacity_ = 0, graph_slots_ = 0, graph_iters_ = 0, graph_tuning_ = -1;
   int graph_smem_ = -1, graph_refill_ = -1, graph_steps_ = -1;
   hpt_status init_status_ = HPT_OK;

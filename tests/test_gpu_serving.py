@@ -162,6 +162,27 @@ def test_graph_replay_equals_eager(scenes):
     assert np.array_equal(a, eager) and np.array_equal(b, eager)
 
 
+def test_graph_replay_follows_a_change_of_scene(scenes):
+    """A batch engine that replays a captured graph bakes the one scene of
+    its jobs into the graph's kernel parameters; running it next on another
+    scene must re-capture, not replay the first scene's pointers."""
+    room, spheres = scenes
+    p = H.make_params(48, 48, 1, 1, (0, 0, 0), 4, 6, 0, 1.0, 5)
+    want = [g.render(S.hp_camera(S.ROOM_CAM), p, want_accum=True)[1] for g in (room, spheres)]
+    t = room.tuning()
+    t.use_graph = 1
+    t.capacity = 1 << 13
+    batch = H.Batch()
+    batch.set_tuning(t)
+    try:
+        for _ in range(2):
+            for g, w in zip((room, spheres), want):
+                batch.add(g, S.hp_camera(S.ROOM_CAM), p, want_accum=True)
+                assert np.array_equal(batch.run()[0][1], w)
+    finally:
+        batch.close()
+
+
 def test_autotune_picks_a_valid_tuning_and_caches_it(scenes):
     spheres = scenes[1]
     t0 = spheres.tuning()
