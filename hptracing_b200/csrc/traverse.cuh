@@ -13,9 +13,13 @@
 // slack (so ties and rounding at leaf faces are still visited). Leaves are
 // still filtered with the reference's own box test on the reference box, so
 // every triangle considered is one the reference would consider.
-// The one reference behaviour not reproduced is its 512-leaf gather cap
-// (kernel.cl:133, 146): a ray whose line pierces more than 512 leaves may
-// lose its true closest hit in the reference, never here.
+// A ray lying exactly in a split plane is walked on both sides of it (see
+// trav_finish). Not reproduced: the reference's 512-leaf gather cap
+// (kernel.cl:133, 146; a ray whose line pierces more than 512 leaves may
+// lose its true closest hit there, never here); exact ties where a ray
+// passes exactly through a leaf's edge or corner (a vertex or edge hit may
+// report another triangle meeting there, at the same t); a zero direction
+// vector, which misses here (the reference reports t = +inf hits).
 #pragma once
 
 #include "checks.cuh"
@@ -116,8 +120,50 @@ struct TravCold {
   int32_t rope;       // node behind the exit face, -1 when there is none
   int32_t pierced;    // reference box test of the leaf: -1 not evaluated yet
   float t_exit;
+  // Rays that lie exactly in a split plane (see trav_finish):
+  float t_start;      // scene entry distance, where every walk starts
+  int32_t ties;       // bits 0-2: axes with a zero direction component;
+                      // 3-5: axes on which a descent met such a plane;
+                      // 6-8: axes whose planes this walk passes on the right
 };
-static_assert(sizeof(TravCold) == 44, "odd word stride in shared memory");
+static_assert(sizeof(TravCold) == 52, "odd word stride in shared memory");
+
+// A ray with a zero direction component whose coordinate equals a node's
+// split on that axis lies in the plane between the two children, and a
+// single stackless walk can only take one side. In the reference a box
+// with that plane as a face gives its slab test 0/0 = NaN and is rejected
+// (_box_intersect, kernel.cl:56-83) unless its inside test holds, i.e. the
+// box contains the ray's origin: so beyond the leaves that contain the
+// origin, both sides of the plane are rejected alike, and only those leaves
+// differ between the sides. The first walk takes the left side of every
+// such plane and records the axes where it met one; if the origin lies in
+// the scene, trav_finish then walks again from the origin once per
+// remaining left/right combination of the zero axes (at most 3 more walks),
+// each only through the leaves that contain the origin, keeping the best
+// hit over all walks. Rays off every split plane walk once.
+HPT_HD bool tie_goes_right(TravCold& tc, uint32_t axis) {
+  tc.ties |= 8 << axis;
+  return (tc.ties >> (6 + axis)) & 1;
+}
+
+// End of a walk: starts the next one if the ray lay in a split plane and a
+// side combination is left (returns false, walk on), else finishes the ray.
+HPT_HD bool trav_finish(TravState& st, TravCold& tc) {
+  const int z = tc.ties & 7, seen = (tc.ties >> 3) & 7, cur = (tc.ties >> 6) & 7;
+  const int next = ((cur | ~z) + 1) & z;  // next subset of z
+  if (seen && next && tc.t_start == 0.f) {
+    tc.ties = z | (seen << 3) | (next << 6);
+    st.node = 0;
+    st.t_entry = 0.f;
+    st.phase = kStepDescend;
+    // Only leaves that contain the origin count on this side: the walk
+    // leaves at the first exit beyond t = 0.
+    tc.t_end = as_float(1);
+    return false;
+  }
+  st.node = -1;
+  return true;
+}
 
 // Work counters of one lane over one kernel launch (summed per warp in 64
 // bits when the launch ends; they feed statistics only).
@@ -141,6 +187,8 @@ HPT_HD void trav_init(const DevScene& s, const Ray& r, TravState& st, TravCold& 
   tc.rope = -1;
   tc.pierced = -1;
   tc.t_exit = 0.f;
+  tc.t_start = 0.f;
+  tc.ties = 0;
   st.steps = 0;
   st.node = -1;
   st.phase = kStepDescend;
@@ -172,14 +220,23 @@ HPT_HD void trav_init(const DevScene& s, const Ray& r, TravState& st, TravCold& 
   st.t_entry = t0;
   tc.t_end = t1;
   tc.slack = rn_div(s.scene_eps, dmax);
+  tc.t_start = t0;
+  tc.ties = (d[0] == 0.f ? 1 : 0) | (d[1] == 0.f ? 2 : 0) | (d[2] == 0.f ? 4 : 0);
   st.node = 0;
   if (start_node > 0 && start_node < s.num_nodes) {
     const uint2 nd = ldg(reinterpret_cast<const uint2*>(s.nodes) + start_node);
     if ((nd.x >> 30) == kLeafKind) {
       const float4* L = reinterpret_cast<const float4*>(s.leaves + (nd.x & kIndexMask));
       const float4 lo = ldg(L), hi = ldg(L + 1);
+      // A hinted start skips the descents from the root, and with them any
+      // split plane the ray lies in; such a plane bounds the leaf, so along a
+      // zero direction component the origin must lie strictly inside.
+      const int z = tc.ties;
+      const bool off_planes = (!(z & 1) || (o[0] > lo.x && o[0] < hi.x)) &&
+                              (!(z & 2) || (o[1] > lo.y && o[1] < hi.y)) &&
+                              (!(z & 4) || (o[2] > lo.z && o[2] < hi.z));
       if (o[0] >= lo.x && o[0] <= hi.x && o[1] >= lo.y && o[1] <= hi.y && o[2] >= lo.z &&
-          o[2] <= hi.z) {
+          o[2] <= hi.z && off_planes) {
         st.node = start_node;
         st.t_entry = 0.f;
       }
@@ -218,7 +275,8 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint
     const float split = as_float_u(nd.y);
     const float p = axis == 0 ? px : (axis == 1 ? py : pz);
     const float dd = axis == 0 ? r.d.x : (axis == 1 ? r.d.y : r.d.z);
-    const bool right = p > split || (p == split && dd > 0.f);
+    const bool right =
+        p > split || (p == split && (dd > 0.f || (dd == 0.f && tie_goes_right(tc, axis))));
     HPT_DCHECK(err, (int)(nd.x & kIndexMask) + 1 < s.num_nodes, 106, nd.x & kIndexMask,
                { st.node = -1; return true; });
     node = (int)(nd.x & kIndexMask) + (right ? 1 : 0);
@@ -318,15 +376,13 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint
   }
   st.steps += 1 + count;
   // Stop once the rest of the ray starts beyond the best hit (+ slack).
-  if (face < 0 || !(t_exit < tc.t_end)) { st.node = -1; return true; }
-  if (st.best.rec >= 0 &&
-      t_exit > rn_add(st.best.t, rn_add(rn_mul(st.best.t, 1e-4f), tc.slack))) {
-    st.node = -1;
-    return true;
-  }
-  const int rope = ldg(reinterpret_cast<const int*>(L) + 8 + face);
-  if (rope < 0 || st.steps > s.max_steps) {
-    if (rope >= 0) hpt_atomic_or(&err->flags, 1u);
+  const int rope = face < 0 ? -1 : ldg(reinterpret_cast<const int*>(L) + 8 + face);
+  if (!(t_exit < tc.t_end) || rope < 0 ||
+      (st.best.rec >= 0 &&
+       t_exit > rn_add(st.best.t, rn_add(rn_mul(st.best.t, 1e-4f), tc.slack))))
+    return trav_finish(st, tc);
+  if (st.steps > s.max_steps) {
+    hpt_atomic_or(&err->flags, 1u);
     st.node = -1;
     return true;
   }
@@ -370,7 +426,8 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, TravCold& tc, const uint
       const float o = axis == 0 ? r.o.x : (axis == 1 ? r.o.y : r.o.z);
       const float dd = axis == 0 ? r.d.x : (axis == 1 ? r.d.y : r.d.z);
       const float p = rn_add(o, rn_mul(st.t_entry, dd));
-      const bool right = p > split || (p == split && dd > 0.f);
+      const bool right =
+        p > split || (p == split && (dd > 0.f || (dd == 0.f && tie_goes_right(tc, axis))));
       HPT_DCHECK(err, (int)(nd.x & kIndexMask) + 1 < s.num_nodes, 106, nd.x & kIndexMask,
                  { st.node = -1; return true; });
       st.node = (int)(nd.x & kIndexMask) + (right ? 1 : 0);
@@ -488,18 +545,13 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, TravCold& tc, const uint
   // (+ slack), else follow the exit rope. A leaf without an exit face has
   // t_exit = +inf and stops here.
   st.phase = kStepDescend;
-  if (!(tc.t_exit < tc.t_end)) {
-    st.node = -1;
-    return true;
-  }
-  if (st.best.rec >= 0 &&
-      tc.t_exit > rn_add(st.best.t, rn_add(rn_mul(st.best.t, 1e-4f), tc.slack))) {
-    st.node = -1;
-    return true;
-  }
   const int rope = tc.rope;
-  if (rope < 0 || st.steps > s.max_steps) {
-    if (rope >= 0) hpt_atomic_or(&err->flags, 1u);
+  if (!(tc.t_exit < tc.t_end) || rope < 0 ||
+      (st.best.rec >= 0 &&
+       tc.t_exit > rn_add(st.best.t, rn_add(rn_mul(st.best.t, 1e-4f), tc.slack))))
+    return trav_finish(st, tc);
+  if (st.steps > s.max_steps) {
+    hpt_atomic_or(&err->flags, 1u);
     st.node = -1;
     return true;
   }

@@ -61,6 +61,17 @@ def test_intersect_bitexact_spheres(spheres, kind):
     _check_intersect(gpu, cpu, o, d)
 
 
+@pytest.mark.parametrize("scene_name", ["room", "spheres"])
+def test_intersect_edge_rays(request, scene_name):
+    """Axis-parallel directions, rays lying in split planes, rays aimed at
+    vertices and shared edges, degenerate rays: the device's closest hits
+    against the oracle under the contract of scenes.check_edge_hits."""
+    mesh, gpu, cpu = request.getfixturevalue(scene_name)
+    for name, (o, d) in S.edge_rays(mesh, cpu.nodes).items():
+        tri, t, u, v = gpu.intersect(o, d)
+        S.check_edge_hits(name, o, d, cpu.intersect(o, d), tri, t, u, v)
+
+
 def test_intersect_secondary_rays(spheres):
     """Rays that start on surfaces (1e-5 off the hit point, as s2 emits)."""
     _, gpu, cpu = spheres

@@ -64,6 +64,20 @@ def test_step_traversal_matches_leaf_traversal(pair, kind):
     assert np.array_equal(a["counts"], b["counts"])
 
 
+@pytest.mark.parametrize("step", [False, True])
+def test_edge_rays_match_oracle(pair, step):
+    """Axis-parallel directions, rays lying in split planes (walked once per
+    side), rays aimed at vertices and shared edges, degenerate rays: the
+    oracle's hits under the contract of scenes.check_edge_hits, in both
+    traversal forms."""
+    cs, em = pair
+    for name, (o, d) in S.edge_rays(cs, cs.nodes).items():
+        got = em.intersect(o, d, step=step)
+        assert got["err"][0] == 0, (name, got["err"])
+        S.check_edge_hits(name, o, d, cs.intersect(o, d), got["tri"], got["t"], got["u"],
+                          got["v"])
+
+
 def test_hinted_secondary_rays_match_oracle(pair):
     """Secondary rays started from the leaf of the previous hit (the kernels'
     start-leaf hint) find the same closest hit as a traversal from the root."""
