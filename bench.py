@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--duration", type=float, default=4.0, help="serve: seconds of arrivals")
     ap.add_argument("--serve-capacity", default=str(1 << 20),
                     help="serve: wavefront capacity (paths in flight; comma list)")
-    ap.add_argument("--large-pct", default="10",
+    ap.add_argument("--large-pct", default="5",
                     help="serve: in-flight cap of the requests larger than the wavefront, "
                          "%% (comma list)")
     ap.add_argument("--depth-ahead", default="1",
