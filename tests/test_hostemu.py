@@ -103,6 +103,32 @@ def test_hinted_secondary_rays_match_oracle(pair):
         assert hinted["counts"][0] <= plain["counts"][0]
 
 
+def test_hints_on_a_split_plane_do_not_hide_the_other_side(pair):
+    """Rays lying in a split plane, each hinted with a leaf that contains its
+    origin, chosen on either side of the plane: a hint whose leaf has the
+    origin on a face along a zero direction component must not be taken (the
+    walk would skip the split planes that need both sides), so the hits stay
+    those of the unhinted walks, under the edge-ray contract."""
+    cs, em = pair
+    o, d = S.edge_rays(cs, cs.nodes, n=500, seed=21)["in_split"]
+    meta, _, leaves = em.tree()
+    leaf_nodes = np.flatnonzero((meta >> 30) == 3)
+    lo = leaves[meta[leaf_nodes] & 0x3FFFFFFF][:, 0:3].view(np.float32)
+    hi = leaves[meta[leaf_nodes] & 0x3FFFFFFF][:, 4:7].view(np.float32)
+    ref = cs.intersect(o, d)
+    for pick in (0, -1):  # first / last leaf (in node order) containing the origin
+        hints = np.full(len(o), -1, np.int32)
+        for i in range(len(o)):
+            inside = np.flatnonzero(((o[i] >= lo) & (o[i] <= hi)).all(axis=1))
+            if inside.size:
+                hints[i] = leaf_nodes[inside[pick]]
+        assert (hints >= 0).mean() > 0.9
+        for step in (False, True):
+            got = em.intersect(o, d, hints=hints, step=step)
+            assert got["err"][0] == 0, got["err"]
+            S.check_edge_hits("in_split", o, d, ref, got["tri"], got["t"], got["u"], got["v"])
+
+
 def test_bad_hints_fall_back_to_root(pair):
     """A hint that is not a leaf node of this tree is ignored."""
     cs, em = pair
