@@ -78,6 +78,18 @@ def test_edge_rays_match_oracle(pair, step):
                           got["v"])
 
 
+def test_edge_rays_same_walks_in_both_forms(pair):
+    """On the edge-ray sets (split-plane walks included) trav_step and
+    trav_leaf report the same hits, the same hit leaves and the same work."""
+    cs, em = pair
+    for name, (o, d) in S.edge_rays(cs, cs.nodes, seed=3).items():
+        a = em.intersect(o, d)
+        b = em.intersect(o, d, step=True)
+        for k in ("tri", "t", "u", "v", "node"):
+            assert np.array_equal(a[k].view(np.int32), b[k].view(np.int32)), (name, k)
+        assert np.array_equal(a["counts"], b["counts"]), name
+
+
 def test_hinted_secondary_rays_match_oracle(pair):
     """Secondary rays started from the leaf of the previous hit (the kernels'
     start-leaf hint) find the same closest hit as a traversal from the root."""
