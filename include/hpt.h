@@ -296,7 +296,11 @@ hpt_status hpt_raygen(const hpt_camera* camera, int32_t sample_x,
 
 /* kdtree_intersect (src/hp/cl_src/kernel.cl:111-208): closest hit per ray.
  * tri_out: triangle id or -1; t_out: hit distance; u_out, v_out: the
- * Moller-Trumbore coordinates of the winning test (0 on a miss). */
+ * Moller-Trumbore coordinates of the winning test (0 on a miss).
+ * Differences from the reference: no 512-leaf gather cap (a ray whose line
+ * pierces more leaves keeps its true closest hit); a ray aimed exactly at a
+ * vertex or edge may report another triangle meeting there at the same t;
+ * a zero direction vector is a miss (the reference reports t = +inf). */
 hpt_status hpt_intersect(hpt_scene* scene, int32_t n, const float* origins,
                          const float* directions, int32_t* tri_out,
                          float* t_out, float* u_out, float* v_out);
