@@ -47,7 +47,9 @@ def parse():
     ap.add_argument("--spp", type=int, default=0)
     # Extra workloads (one JSON line each): the 32-job mixed batch, batched
     # vs one job at a time; the Poisson serving stream.
-    ap.add_argument("--mode", default="frame", choices=["frame", "batch", "serve"])
+    ap.add_argument("--mode", default="frame", choices=["frame", "batch", "serve", "compact"])
+    ap.add_argument("--compact-n", type=int, default=1 << 25,
+                    help="compact: number of flags")
     ap.add_argument("--scene", default="spheres", choices=["spheres", "terrain"],
                     help="frame: the 61k-triangle spheres frame (headline) or the "
                          "2.4M-triangle terrain at 1920x1080, 256 spp")
@@ -175,7 +177,7 @@ SCENE = "spheres"
 
 def make_scene():
     import hptracing_b200 as H
-    from tests import scenes as S
+    from hptracing_b200 import scenes as S
     if SCENE == "terrain":
         mesh = H.Mesh.generate(2, seed=2)
         nodes, leaf = H.build_kdtree(mesh.points, mesh.triangles)
@@ -288,7 +290,7 @@ def run_batch(args):
     import hptracing_b200 as H
     from hptracing_b200 import build as hbuild
     from hptracing_b200 import shard
-    from tests import scenes as S
+    from hptracing_b200 import scenes as S
     rank, world, local = dist_setup(args.gpus)
     hbuild.build()
     torch.cuda.set_device(local)
@@ -386,7 +388,7 @@ def run_serve(args):
     import torch
     import hptracing_b200 as H
     from hptracing_b200 import build as hbuild
-    from tests import scenes as S
+    from hptracing_b200 import scenes as S
     hbuild.build()
     torch.cuda.set_device(0)
     t0 = time.perf_counter()
@@ -515,9 +517,85 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, args, capacity, large_
     server.close()
 
 
+def run_compact(args):
+    """Standalone stream compaction (the stage ABI's stable compaction
+    kernels: per-tile counts, one-block scan, scatter). Device-resident
+    flags of n = 2^25 u32 (128 MiB, survivors with probability 1/2), timed
+    with CUDA events on the launching stream, L2 flushed between calls.
+    Algorithmic bytes: 4 per flag read + 4 per survivor index written."""
+    import ctypes as C
+
+    import torch
+    import hptracing_b200 as H
+    from hptracing_b200 import _lib
+    from hptracing_b200 import build as hbuild
+    hbuild.build()
+    torch.cuda.set_device(0)
+    n = args.compact_n
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0x48505400)
+    flags = (torch.rand(n, device="cuda", generator=g) < 0.5).to(torch.int32)
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    L = _lib.lib()
+    stream = torch.cuda.current_stream()
+
+    def call():
+        _lib.check(L.hpt_compact_noalloc(C.c_void_p(flags.data_ptr()), n,
+                                         C.c_void_p(out.data_ptr()), C.c_void_p(cnt.data_ptr()),
+                                         C.c_void_p(stream.cuda_stream)))
+
+    for _ in range(args.warmup):
+        call()
+    torch.cuda.synchronize()
+    times = []
+    sampler = ClockSampler(0)
+    sampler.start()
+    for _ in range(args.steps):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        call()
+        b.record(stream)
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    clocks = sampler.stop()
+    total = int(cnt.item())
+    ref = torch.nonzero(flags).flatten().to(torch.int32)
+    exact = total == ref.numel() and bool(torch.equal(out[:total], ref))
+    ms = statistics.median(times)
+    alg = 4.0 * n + 4.0 * total
+    peak, peak_kind = measured_peak()
+    # End to end through the host-array entry point (copies in and out).
+    hflags = flags.cpu().numpy().astype(np.uint32)
+    walls = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        H.compact(hflags)
+        walls.append(time.perf_counter() - t0)
+    line = {"metric": "compaction GB/s", "mode": "compact", "value": alg / (ms / 1e3) / 1e9,
+            "unit": "GB/s", "n": n, "survivors": total, "exact": exact,
+            "ms_per_call": ms, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True,
+            "roofline": {"bound": "hbm", "kernel": "k_compact_count+scan+scatter",
+                         "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_call": alg},
+            "e2e": {"value": n / statistics.median(walls) / 1e9, "unit": "Gflags/s",
+                    "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 4 * total + 4},
+            "l2": "flushed between calls (512 MiB write)", "clocks": clocks,
+            "dtype": "u32", "data": "synthetic (seeded flags, p = 0.5)"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     global W_RES, H_RES, SPP, WORKLOAD, SCENE, BG
     args = parse()
+    if args.mode == "compact":
+        run_compact(args)
+        return
     if args.mode == "batch":
         run_batch(args)
         if int(os.environ.get("WORLD_SIZE", "1")) > 1:
@@ -550,7 +628,7 @@ def main():
     torch.cuda.set_device(local)
     mesh, nodes, leaf, cam = make_scene()
     scene = H.Scene(mesh, nodes, leaf, device=local)
-    from tests import scenes as S
+    from hptracing_b200 import scenes as S
     camera = S.hp_camera(cam)
     tune = scene.tuning()
     tune.profile = 1

@@ -766,6 +766,14 @@ hpt_tuning default_tuning() {
   return t;
 }
 
+// The scene as a job sees it: the tuning's step cap, when set, replaces the
+// scene's own (only ever lowering it).
+DevScene capped_scene(const DevScene& s, const hpt_tuning& t) {
+  DevScene out = s;
+  if (t.max_steps > 0) out.max_steps = std::min(out.max_steps, t.max_steps);
+  return out;
+}
+
 hpt_status check_render_params(const hpt_camera* cam, const hpt_render_params* p) {
   if (!cam || !p) return fail(HPT_ERR_INVALID_ARGUMENT, "camera/params is NULL");
   if (p->sample_x <= 0 || p->sample_y <= 0 || p->supersample_x <= 0 || p->supersample_y <= 0 ||
@@ -1030,7 +1038,7 @@ DevJob Engine::make_job(const JobSpec& js, const JobBuffers& b) const {
   memset(&j, 0, sizeof j);
   const hpt_camera& cam = js.camera;
   const hpt_render_params& p = js.params;
-  j.scene = js.scene->dev;
+  j.scene = capped_scene(js.scene->dev, tuning);
   for (int k = 0; k < 3; ++k) {
     j.view_p[k] = cam.view_p[k];
     j.top[k] = cam.top_dir[k];
@@ -1090,7 +1098,7 @@ static EngineParams make_params(const Engine& e, DevCtrl* ctrl, DevJob* jobs, De
   P.trav_steps = std::max(0, e.tuning.trav_steps);
   if (shared) {
     P.uniform_scene = 1;
-    P.uscene = *shared;
+    P.uscene = capped_scene(*shared, e.tuning);
   }
   if (shared && e.tuning.smem_nodes > 0) {
     P.smem_nodes = std::min(e.tuning.smem_nodes, shared->num_nodes);
@@ -1279,7 +1287,7 @@ hpt_status Engine::ensure_graph(const DevScene* shared_scene, int iterations) {
   if (graph_exec_ && same_scene && graph_capacity_ == capacity_ &&
       graph_slots_ == slots_ && graph_iters_ == iterations && graph_tuning_ == isect_variant() &&
       graph_smem_ == tuning.smem_nodes && graph_refill_ == tuning.refill_chunk &&
-      graph_steps_ == tuning.trav_steps)
+      graph_steps_ == tuning.trav_steps && graph_max_steps_ == tuning.max_steps)
     return HPT_OK;
   if (graph_exec_) {
     HPT_SOFT(cudaGraphExecDestroy(graph_exec_));
@@ -1307,6 +1315,7 @@ hpt_status Engine::ensure_graph(const DevScene* shared_scene, int iterations) {
   graph_smem_ = tuning.smem_nodes;
   graph_refill_ = tuning.refill_chunk;
   graph_steps_ = tuning.trav_steps;
+  graph_max_steps_ = tuning.max_steps;
   return HPT_OK;
 }
 

@@ -157,7 +157,7 @@ class Engine {
   bool graph_shared_ = false;
   DevScene graph_scene_{};
   int graph_capacity_ = 0, graph_slots_ = 0, graph_iters_ = 0, graph_tuning_ = -1;
-  int graph_smem_ = -1, graph_refill_ = -1, graph_steps_ = -1;
+  int graph_smem_ = -1, graph_refill_ = -1, graph_steps_ = -1, graph_max_steps_ = -1;
   hpt_status init_status_ = HPT_OK;
   hpt_status init();
   int occ_isect_ = 1, occ_shade_ = 1;
@@ -176,6 +176,7 @@ struct SceneHandle {
 hpt_status upload_scene(const hpt_scene_desc& desc, SceneDev& out);
 void release_scene(SceneDev& s);
 hpt_tuning default_tuning();
+DevScene capped_scene(const DevScene& s, const hpt_tuning& t);
 hpt_status check_render_params(const hpt_camera* cam, const hpt_render_params* p);
 
 // CUDA error -> hpt_status with message.

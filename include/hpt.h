@@ -276,6 +276,11 @@ typedef struct hpt_tuning {
                              /* n traversal steps (descent step, leaf     */
                              /* set-up, triangle test or leaf exit) per   */
                              /* lane between refills                      */
+  int32_t max_steps;         /* traversal steps one ray may take before   */
+                             /* the walk gives up and the render returns  */
+                             /* HPT_ERR_TRAVERSAL_LIMIT; 0 = the scene's  */
+                             /* cap, 8 x (nodes + leaf references) +      */
+                             /* 100000. Larger values are clamped to it.  */
 } hpt_tuning;
 hpt_status hpt_tuning_get(const hpt_scene* scene, hpt_tuning* out);
 hpt_status hpt_tuning_set(hpt_scene* scene, const hpt_tuning* in);

@@ -4,8 +4,9 @@
 
 1. oracle/liboracle.so from oracle/hpt_oracle.cpp: the CPU restatement of
    the reference path (always built; it is the oracle).
-2. When the reference sources are present (REFERENCE_ROOT, default
-   /root/reference), oracle/_ref/ receives:
+2. When the reference sources are present (the directory named by
+   REFERENCE_ROOT, else the container's read-only mount /root/reference if
+   it exists), oracle/_ref/ receives:
      - librefcl.so: the reference's src/hp/cl_src/kernel.cl compiled as C++
        through refshim/opencl_c.h, driven by refcl_driver.cpp. The only
        change made to the kernel source on the way is a mechanical rewrite of
@@ -32,8 +33,16 @@ REFSCENE_LIB = os.path.join(REF_OUT, "librefscene.so")
 FLAGS = ["-O2", "-std=c++14", "-fPIC", "-shared", "-pthread", "-ffp-contract=off"]
 
 
+DEFAULT_REFERENCE_MOUNT = "/root/reference"
+
+
 def reference_root():
-    return os.environ.get("REFERENCE_ROOT", "/root/reference")
+    """Directory of the reference sources, or None where they are absent
+    (GPU hosts run only the prebuilt oracle/_ref files)."""
+    root = os.environ.get("REFERENCE_ROOT")
+    if root:
+        return root if os.path.isdir(root) else None
+    return DEFAULT_REFERENCE_MOUNT if os.path.isdir(DEFAULT_REFERENCE_MOUNT) else None
 
 
 def _run(cmd):
@@ -58,6 +67,8 @@ def build_oracle():
 
 def build_reference():
     root = reference_root()
+    if root is None:
+        return None
     kernel = os.path.join(root, "src", "hp", "cl_src", "kernel.cl")
     types = os.path.join(root, "src", "hp", "cl_src", "types.h.cl")
     if not (os.path.exists(kernel) and os.path.exists(types)):

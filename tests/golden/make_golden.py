@@ -1,7 +1,8 @@
 """Generates the golden fixtures in tests/golden/ from the reference itself.
 
-Run where the reference sources are mounted (default /root/reference, or
-REFERENCE_ROOT) after `python -m oracle.build` has built oracle/_ref/:
+Run where the reference sources are present (REFERENCE_ROOT, or the mount
+oracle.build.reference_root() finds) after `python -m oracle.build` has
+built oracle/_ref/:
 
     python tests/golden/make_golden.py
 
@@ -19,6 +20,16 @@ Fixtures (all outputs of the reference's own code or tests):
                        (kernel.cl compiled as C++) on the box-room scene:
                        raygen, kdtree_intersect, s1_run, s2_*_run, get_image
   render_room.npz      a small TraceRunner::run-equivalent render
+  cornell_box.npz      the embree Cornell box (scene/simple-cornell-box/
+                       cornell_box.obj) as the reference's own loader and
+                       SAH builder produce it (hp::KDTree: points, normals,
+                       texcoords, triangles, materials, lights, getData()),
+                       plus the reference kernels' estimate of its image
+                       (kernel.cl compiled as C++, one host thread, per-lane
+                       LCG as TraceRunner::run draws it) with per-ray sums
+                       of squares from the oracle's bit-identical run
+
+    python tests/golden/make_golden.py [--only cornell]
 """
 import hashlib
 import json
@@ -37,7 +48,11 @@ import oracle as O  # noqa: E402
 from tests import scenes as S  # noqa: E402
 from tests import objio  # noqa: E402
 
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+from oracle import build as obuild  # noqa: E402
+
+REF = obuild.reference_root()
+if REF is None:
+    raise SystemExit("reference sources not found: set REFERENCE_ROOT")
 
 
 def parse_box_cases():
@@ -86,9 +101,45 @@ KD_SCENES = [("room", dict(config=0, seed=0)),
              ("room_tess", dict(config=3, seed=7, family=0, target_triangles=2000))]
 
 
+# Camera of the Cornell fixture: the embree scene's usual viewpoint, with the
+# reference CLI's conventions (forward = up x right, image-plane height =
+# --angle at unit distance, src/hptracing.cpp:74-78).
+CORNELL_CAM = dict(view_p=(278.0, 273.0, -800.0), top_dir=(0.0, 1.0, 0.0),
+                   right_dir=(-1.0, 0.0, 0.0), width=0.68, height=0.68)
+# Readme.md:53-55 renders it at 500 x 500, 50 samples, depth 5; the fixture
+# keeps that camera and depth on a 100 x 100 raster, 256 samples per ray.
+CORNELL_RES, CORNELL_SPP, CORNELL_DEPTH, CORNELL_SEED = 100, 256, 5, 77
+
+
+def cornell_fixture():
+    cb = os.path.join(REF, "scene", "simple-cornell-box", "cornell_box.obj")
+    r = O.ref_load_scene(cb, os.path.dirname(cb) + "/")
+    mesh = H.Mesh(r["points"], r["triangles"], r["materials"], r["normals"], r["texcoords"],
+                  r["lights"])
+    cs = O.CpuScene(mesh, r["nodes"], r["leaf_data"])
+    w = CORNELL_RES
+    acc, rgba, counts = cs.refcl_render(CORNELL_CAM, w, w, 1, 1, (0, 0, 0), CORNELL_SPP,
+                                        CORNELL_DEPTH, 0, 1.0, seed=CORNELL_SEED, threads=1)
+    acc_o, acc2, counts_o = cs.render(CORNELL_CAM, w, w, 1, 1, (0, 0, 0), CORNELL_SPP,
+                                      CORNELL_DEPTH, 0, seed=CORNELL_SEED, rng_mode=0, threads=1)
+    assert np.array_equal(acc, acc_o) and counts[0] == counts_o[0], "oracle != reference kernels"
+    np.savez_compressed(os.path.join(HERE, "cornell_box.npz"),
+                        points=r["points"], normals=r["normals"], texcoords=r["texcoords"],
+                        triangles=r["triangles"], materials=r["materials"], lights=r["lights"],
+                        nodes=r["nodes"], leaf_data=r["leaf_data"],
+                        camera=np.array(list(CORNELL_CAM["view_p"]) + list(CORNELL_CAM["top_dir"])
+                                        + list(CORNELL_CAM["right_dir"]) +
+                                        [CORNELL_CAM["width"], CORNELL_CAM["height"]], np.float32),
+                        res=w, spp=CORNELL_SPP, depth=CORNELL_DEPTH, seed=CORNELL_SEED,
+                        ref_accum=acc, ref_accum_sq=acc2, ref_rgba=rgba, ref_queries=counts[0])
+
+
 def main():
     from oracle import build as obuild
     obuild.build()
+    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "cornell":
+        cornell_fixture()
+        return
     assert O.refcl_lib() is not None and O.refscene_lib() is not None, "reference not built"
     out = {}
     cases = parse_box_cases()
@@ -154,6 +205,7 @@ def main():
                                         threads=1)
     np.savez_compressed(os.path.join(HERE, "render_room.npz"), accum=acc, rgba=rgba,
                         counts=counts)
+    cornell_fixture()
     print("golden fixtures written to", HERE)
 
 

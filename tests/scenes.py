@@ -1,33 +1,9 @@
-"""Seeded test scenes and cameras shared by the tests."""
-import math
+"""Seeded test ray sets shared by the tests (the scenes and cameras live in
+hptracing_b200.scenes)."""
 
 import numpy as np
 
-import hptracing_b200 as H
-
-# Box-room camera: eye (0.5, 0.5, -1.4), forward = up x right = +z, 40 deg.
-ROOM_CAM = dict(view_p=(0.5, 0.5, -1.4), top_dir=(0.0, 1.0, 0.0), right_dir=(-1.0, 0.0, 0.0),
-                width=2 * math.tan(math.radians(20)), height=2 * math.tan(math.radians(20)))
-# Panorama from inside the room (height < 0 selects set_viewdirs_vr).
-PANO_CAM = dict(view_p=(0.5, 0.5, 0.5), top_dir=(0.0, 1.0, 0.0), right_dir=(0.0, 0.0, 1.0),
-                width=1.0, height=-1.0)
-
-
-def terrain_cam(aspect=16 / 9):
-    a = math.radians(25)
-    h = 2 * math.tan(a)
-    return dict(view_p=(0.0, 0.9, -1.6), top_dir=(0.0, math.cos(a), math.sin(a)),
-                right_dir=(-1.0, 0.0, 0.0), width=aspect * h, height=h)
-
-
-def hp_camera(c):
-    return H.make_camera(c["view_p"], c["top_dir"], c["right_dir"], c["width"], c["height"])
-
-
-def make_scene(config, seed=0, **kw):
-    mesh = H.Mesh.generate(config, seed=seed, **kw)
-    nodes, leaf = H.build_kdtree(mesh.points, mesh.triangles)
-    return mesh, nodes, leaf
+from hptracing_b200.scenes import PANO_CAM, ROOM_CAM, hp_camera, make_scene, terrain_cam  # noqa: F401
 
 
 def random_rays(n, seed, lo=-0.1, hi=1.1):
@@ -113,3 +89,50 @@ def check_edge_hits(name, o, d, ref, tri, t, u, v):
         assert (tri[zero] < 0).all()
     else:
         assert bad.sum() == 0, (name, np.flatnonzero(bad)[:5])
+
+
+def aabb_random_rays(mesh, n, seed, pad=0.1):
+    """Origins uniform in the scene's bounding box grown by `pad` of its
+    extent on every side, directions uniform on the sphere."""
+    lo, hi = mesh.points[:, :3].min(0), mesh.points[:, :3].max(0)
+    g = pad * (hi - lo)
+    rng = np.random.default_rng(seed)
+    o = rng.uniform(lo - g, hi + g, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return o, d.astype(np.float32)
+
+
+def oracle_bounce_rays(cpu, o, d, bounces, seed, threads=None):
+    """The rays the oracle sends to its intersect stage after `bounces`
+    shading passes (s1_run + s2_*_run) that start from rays (o, d) with
+    strength 1 and seeded 48-bit LCG states; every stage is the oracle's."""
+    rng = np.random.default_rng(seed)
+    st = np.ones((len(o), 3), np.float32)
+    sd = rng.integers(0, 2 ** 48, len(o), dtype=np.int64)
+    kw = {} if threads is None else dict(threads=threads)
+    for _ in range(bounces):
+        r = cpu.intersect(o, d, **kw)
+        h = r["tri"] >= 0
+        sh = cpu.shade(o[h], d[h], st[h], r["tri"][h], r["t"][h], sd[h])
+        a = sh["branch"] >= 0
+        nd = cpu.next_dir(sh["branch"][a], d[h][a], sh["hit_p"][a], sh["normal"][a],
+                          sh["strength"][a], sh["param"][a], sh["seeds"][a])
+        k = nd["alive"] == 1
+        o, d, st, sd = nd["origins"][k], nd["directions"][k], nd["strength"][k], nd["seeds"][k]
+    return np.ascontiguousarray(o), np.ascontiguousarray(d)
+
+
+def hit_parity(ref, tri, t, u, v):
+    """Closest hits of the device against the oracle. Returns counts:
+    rays, hits, `cap` (rays past the reference's 512-leaf gather cap, not
+    compared), `ties` (another triangle at the bit-identical t: a ray
+    through a shared edge or vertex) and `other` (any other difference)."""
+    ok = ref["overflow"] == 0
+    diff = ok & ((ref["tri"] != tri) | (ref["t"].view(np.int32) != t.view(np.int32)) |
+                 (ref["u"].view(np.int32) != u.view(np.int32)) |
+                 (ref["v"].view(np.int32) != v.view(np.int32)))
+    tie = diff & (ref["t"].view(np.int32) == t.view(np.int32)) & (ref["tri"] >= 0) & (tri >= 0)
+    return dict(rays=int(len(tri)), hits=int((ref["tri"] >= 0).sum()), cap=int((~ok).sum()),
+                ties=int(tie.sum()), other=int((diff & ~tie).sum()),
+                first_other=np.flatnonzero(diff & ~tie)[:5].tolist())

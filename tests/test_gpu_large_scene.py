@@ -1,11 +1,19 @@
 """The large scene (terrain: 1024x1024-vertex heightfield + 16 columns,
-2.4M triangles, eight 2048^2 textures) on the GPU.
+2.4M triangles, eight 2048^2 textures: the benchmarked terrain frame's
+scene) on the GPU.
 
-At full size the oracle still intersects a few ten thousand rays in
-seconds, so closest hits are compared bit for bit there; whole renders are
-compared with the oracle on a reduced terrain (256^2 heightfield, 450k
-triangles) and checked at full size through properties that do not depend
-on size: determinism, batch == alone, no device check or step cap firing."""
+At full size the oracle intersects 2^20 rays in seconds, so closest hits
+are compared bit for bit on 2^20 camera rays, 2^20 random rays and the
+oracle's own bounce-2 secondary rays (counting shared-edge ties: the
+regular heightfield grid puts a few camera rays exactly on a shared edge,
+where another triangle at the bit-identical t may be reported). Whole
+renders are compared with the counter-mode oracle at full size (reduced
+resolution and spp) and on a reduced terrain (256^2 heightfield, 450k
+triangles), and checked at full size through properties that do not
+depend on size: determinism, batch == alone, no device check or step cap
+firing."""
+import os
+
 import numpy as np
 import pytest
 
@@ -16,10 +24,12 @@ from tests import scenes as S
 pytestmark = pytest.mark.gpu
 
 CAM = S.terrain_cam(16 / 9)
+THREADS = max(1, os.cpu_count() or 1)
+N = 1 << 20
 
 
-def _terrain(n):
-    mesh = H.Mesh.generate(2, seed=2, heightfield_n=n, texture_size=256)
+def _terrain(n, texture_size=256):
+    mesh = H.Mesh.generate(2, seed=2, heightfield_n=n, texture_size=texture_size)
     nodes, leaf = H.build_kdtree(mesh.points, mesh.triangles)
     return mesh, nodes, leaf
 
@@ -28,8 +38,9 @@ def _terrain(n):
 def full(built):
     if H.device_count() == 0:
         pytest.skip("no CUDA device")
-    mesh, nodes, leaf = _terrain(1024)
-    assert len(mesh.triangles) > 2_000_000
+    mesh, nodes, leaf = _terrain(1024, texture_size=0)  # nominal: eight 2048^2 textures
+    assert len(mesh.triangles) > 2_400_000
+    assert mesh.texture_dims.tolist() == [[2048, 2048]] * 8
     return mesh, H.Scene(mesh, nodes, leaf), O.CpuScene(mesh, nodes, leaf)
 
 
@@ -41,29 +52,48 @@ def small(built):
     return mesh, H.Scene(mesh, nodes, leaf), O.CpuScene(mesh, nodes, leaf)
 
 
-def _same_hits(ref, got):
-    ok = ref["overflow"] == 0
-    assert ok.mean() > 0.999
-    for k in ("tri", "t", "u", "v"):
-        a, b = np.asarray(ref[k])[ok], np.asarray(got[k])[ok]
-        bad = np.flatnonzero(a.view(np.int32) != b.view(np.int32))
-        assert bad.size == 0, (k, bad[:5])
-
-
-def test_full_size_closest_hits_bitexact(full):
+@pytest.mark.parametrize("kind", ["camera", "random", "secondary"])
+def test_full_size_closest_hits_2pow20(full, kind):
+    """2^20-ray batches on the full terrain: bit-exact closest hits except
+    shared-edge ties (another triangle at the bit-identical t), which are
+    counted and bounded at 1e-5 of the rays."""
     mesh, gpu, cpu = full
-    o1, d1 = O.raygen(CAM, 480, 270, 1, 1)
-    rng = np.random.default_rng(17)
-    lo, hi = mesh.points[:, :3].min(0), mesh.points[:, :3].max(0)
-    o2 = rng.uniform(lo - 0.1, hi + 0.1, (20000, 3)).astype(np.float32)
-    d2 = rng.normal(size=(20000, 3)).astype(np.float32)
-    d2 /= np.linalg.norm(d2, axis=1, keepdims=True)
-    for o, d in ((o1, d1), (o2, d2)):
-        ref = cpu.intersect(o, d)
-        tri, t, u, v = gpu.intersect(o, d)
-        got = dict(tri=tri, t=t, u=u, v=v)
-        _same_hits(ref, got)
-    assert (got["tri"] >= 0).mean() > 0.3
+    o, d = O.raygen(CAM, 1366, 768, 1, 1)
+    o, d = np.ascontiguousarray(o[:N]), np.ascontiguousarray(d[:N])
+    if kind == "random":
+        o, d = S.aabb_random_rays(mesh, N, seed=0x48505402)
+    elif kind == "secondary":
+        o, d = S.oracle_bounce_rays(cpu, o, d, 2, seed=3, threads=THREADS)
+    ref = cpu.intersect(o, d, threads=THREADS)
+    tri, t, u, v = gpu.intersect(o, d)
+    c = S.hit_parity(ref, tri, t, u, v)
+    print("C2 %s: %d rays, %d hits, cap cases %d, shared-edge ties %d, other differences %d"
+          % (kind, c["rays"], c["hits"], c["cap"], c["ties"], c["other"]))
+    assert c["other"] == 0, c["first_other"]
+    assert c["ties"] <= 1e-5 * c["rays"]
+    assert c["cap"] <= 1e-3 * c["rays"]
+    assert c["hits"] > 0.3 * c["rays"] if kind == "camera" else c["hits"] > 0
+
+
+def test_full_size_render_matches_counter_oracle(full):
+    """The full 2.4M-triangle terrain frame at reduced resolution and spp
+    (128 x 72, 2 spp, depth 8, environment 0.2) against the oracle driven
+    by the same random streams."""
+    _, gpu, cpu = full
+    w, h, spp, depth, bg = 128, 72, 2, 8, (0.2, 0.2, 0.2)
+    p = H.make_params(w, h, 1, 1, bg, spp, depth, 0, 1.0, 5)
+    _, acc = gpu.render(S.hp_camera(CAM), p, want_accum=True)
+    st = gpu.stats()
+    ref, _, counts = cpu.render(CAM, w, h, 1, 1, bg, spp, depth, 0, seed=5, rng_mode=1,
+                                threads=THREADS)
+    rel = np.abs(acc - ref) / (np.abs(ref) + 1e-3)
+    bad = (rel > 1e-3).any(axis=1).mean()
+    print("C2 full terrain: rays off by >1e-3: %.4f; queries gpu %d oracle %d"
+          % (bad, st["intersect_queries"], counts[0]))
+    assert bad < 0.02
+    assert abs(acc.sum() - ref.sum()) / ref.sum() < 0.01
+    assert abs(st["intersect_queries"] - counts[0]) / counts[0] < 0.01
+    assert st["error_flags"] == 0
 
 
 def test_reduced_terrain_render_matches_counter_oracle(small):

@@ -200,3 +200,32 @@ def test_cli_replays_gui_camera_keys(built, tmp_path):
         frames.append(np.frombuffer(data[len(b"P6\n48 32\n255\n"):], np.uint8))
     assert not os.path.exists(str(tmp_path / "cam_003.ppm"))
     assert np.abs(frames[1].astype(int) - frames[0].astype(int)).mean() > 1.0
+
+
+def test_step_cap_returns_traversal_limit(room):
+    """Failure detection of the bounded traversal: with the per-ray step cap
+    lowered to 3 every walk runs out, ends its ray and sets the cap flag; the
+    kernels still drain (the call returns) and the render reports
+    HPT_ERR_TRAVERSAL_LIMIT. The next render with the scene's own cap is
+    bit-identical to one made before."""
+    _, gpu, _ = room
+    cam = S.hp_camera(S.ROOM_CAM)
+    p = H.make_params(32, 24, 1, 1, (0.1, 0.1, 0.1), 2, 5, 0, 1.0, 3)
+    before = gpu.render(cam, p, want_accum=True)[1]
+    saved = gpu.tuning()
+    t = gpu.tuning()
+    t.max_steps = 3
+    gpu.set_tuning(t)
+    try:
+        with pytest.raises(H.HptError) as e:
+            gpu.render(cam, p, want_accum=True)
+        assert e.value.status == 5  # HPT_ERR_TRAVERSAL_LIMIT
+        assert "step cap" in str(e.value)
+        st = gpu.stats()
+        assert st["error_flags"] & 1
+        assert st["intersect_queries"] >= 32 * 24
+    finally:
+        gpu.set_tuning(saved)
+    after = gpu.render(cam, p, want_accum=True)[1]
+    assert gpu.stats()["error_flags"] == 0
+    assert np.array_equal(before, after)

@@ -17,11 +17,12 @@ import pytest
 
 import hptracing_b200 as H
 import oracle as O
+from oracle import build as obuild
 from tests import objio
 from tests import scenes as S
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = obuild.reference_root() or "<reference sources absent>"
 CORNELL = os.path.join(REF, "scene", "simple-cornell-box", "cornell_box.obj")
 
 
