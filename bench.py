@@ -14,6 +14,18 @@ e2e:   the same queries / host wall time of the hpt_render C-ABI calls,
        which include the job upload and the RGBA read-back.
 With N > 1 each rank renders its own frames (independent jobs, no
 collective): weak scaling.
+
+The default line also carries the metric's other two parts, measured after
+the frames: "batch" (the 32 mixed jobs one by one through hpt_render vs in
+one hpt_batch wavefront; accumulators bit-identical, so equal relMSE) and,
+at N = 1, "serve" (the Poisson stream over four resident scenes at 50
+requests/s: pose and panorama p50/p99). --frame-only leaves them out.
+Other modes print their own line: --mode batch | serve | compact.
+
+--impl reference: the reference's own kernels (kernel.cl compiled as C++)
+on the host cores, on the same frame's scene as the reference's own loader
+and SAH builder build it from the stored workload file, without the
+product library.
 """
 import argparse
 import json
@@ -42,6 +54,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--frame-only", action="store_true",
+                    help="frame: leave out the batch and serving parts of the default line")
+    ap.add_argument("--serve-seconds", type=float, default=4.0,
+                    help="frame: seconds of arrivals of the serving part")
     # Overrides for profiling runs only (the headline workload is the default).
     ap.add_argument("--res", type=int, default=0)
     ap.add_argument("--spp", type=int, default=0)
@@ -175,6 +191,41 @@ def profiled_traffic():
 SCENE = "spheres"
 
 
+# The headline frame's scene as a file: written at build time by the
+# product's generator (write_reference_workload), read by the reference arm,
+# which never loads the product library: it rebuilds the scene's KD-tree
+# with the reference's own loader and SAH builder from this file.
+WORKLOAD_FILE = os.path.join(ROOT, "oracle", "_ref", "workload_spheres64_61k.npz")
+_MESH_KEYS = ("points", "normals", "texcoords", "triangles", "materials", "lights",
+              "texture_data", "texture_dims")
+
+
+def write_reference_workload(path=None, force=False):
+    """Stores the spheres frame's scene (hpt_mesh_generate config 1, seed 1:
+    geometry, materials, light table and the four 1024^2 RGBA8 texture
+    layers) for the reference arm. Called by __graft_entry__.build()."""
+    import hptracing_b200 as H
+    from hptracing_b200 import build as hbuild
+    path = path or WORKLOAD_FILE
+    if (not force and os.path.exists(path) and
+            os.path.getmtime(path) >= os.path.getmtime(hbuild.LIB)):
+        return path
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    mesh = H.Mesh.generate(1, seed=1)
+    tmp = path + ".tmp.npz"
+    np.savez(tmp, **{k: getattr(mesh, k) for k in _MESH_KEYS})
+    os.replace(tmp, path)
+    return path
+
+
+class _StoredMesh:
+    """hp::Scene arrays read from the stored workload file."""
+
+    def __init__(self, data, **override):
+        for k in _MESH_KEYS:
+            setattr(self, k, override.get(k, data[k]))
+
+
 def make_scene():
     import hptracing_b200 as H
     from hptracing_b200 import scenes as S
@@ -184,6 +235,34 @@ def make_scene():
         return mesh, nodes, leaf, S.terrain_cam(W_RES / H_RES)
     mesh, nodes, leaf = S.make_scene(1, seed=1)
     return mesh, nodes, leaf, S.ROOM_CAM
+
+
+def reference_scene():
+    """The spheres frame's scene for the reference arm, without the product
+    library: the stored workload's geometry and materials are written as
+    OBJ + MTL and loaded by the reference's own hp::KDTree (its OBJ loader,
+    material probabilities, light table and SAH builder, compiled from the
+    reference sources into oracle/_ref/librefscene.so). The reference decodes
+    texture maps through ImageMagick, which is absent here, so the texture
+    ids and RGBA8 layers are attached from the stored workload, as
+    TraceRunner uploads them (trace_runner.cpp:67-86)."""
+    import tempfile
+
+    import oracle as O
+    from oracle import objio
+    data = np.load(WORKLOAD_FILE)
+    stored = _StoredMesh(data)
+    with tempfile.TemporaryDirectory() as d:
+        path = objio.write_obj(stored, d, "spheres64")
+        r = O.ref_load_scene(path, d + "/")
+    if r is None:
+        raise RuntimeError("the reference's scene library is not built")
+    mats = r["materials"].copy()
+    mats["diffuse_texture_id"] = data["materials"]["diffuse_texture_id"]
+    mats["ambient_texture_id"] = data["materials"]["ambient_texture_id"]
+    mesh = _StoredMesh(data, points=r["points"], normals=r["normals"], texcoords=r["texcoords"],
+                       triangles=r["triangles"], materials=mats, lights=r["lights"])
+    return mesh, r["nodes"], r["leaf_data"]
 
 
 def isect_bytes(stats):
@@ -213,35 +292,99 @@ def cpu_baseline(mesh, nodes, leaf, cam, kind):
                                  rng_mode=0, threads=threads)
     dt = time.perf_counter() - t0
     return {"value": counts[0] / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": kind,
+            "seconds": dt,
             "sample": "%dx%d rays x 1 sample x depth %d of the same frame (%d queries, %.1f s)"
                       % (W_RES, H_RES, DEPTH, int(counts[0]), dt)}
 
 
 def run_reference(args):
+    """The reference arm: the reference's own kernels (kernel.cl compiled as
+    C++, driven like TraceRunner::run) on all host cores, on the spheres
+    frame's scene as the reference's own loader and SAH builder build it.
+    Each step is a bounded sample of the frame (1 of its 64 samples per ray);
+    the metric (intersect queries per second) is the same as the GPU arm's."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     import oracle as O
     from oracle import build as obuild
     obuild.build()
-    kind = "reference" if O.refcl_lib() is not None else "port"
-    mesh, nodes, leaf, cam = make_scene()
+    if O.refcl_lib() is None or O.refscene_lib() is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the reference kernels were not built (oracle/_ref missing)"}))
+        return
+    if not os.path.exists(WORKLOAD_FILE):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "workload file missing (written by __graft_entry__.build())"}))
+        return
+    from hptracing_b200 import scenes as S
+    t0 = time.perf_counter()
+    mesh, nodes, leaf = reference_scene()
+    build_s = time.perf_counter() - t0
+    cam = S.ROOM_CAM
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     for _ in range(args.warmup):
-        cpu_baseline(mesh, nodes, leaf, cam, kind)
-    vals = [cpu_baseline(mesh, nodes, leaf, cam, kind) for _ in range(args.steps)]
+        cpu_baseline(mesh, nodes, leaf, cam, "reference")
+    vals = [cpu_baseline(mesh, nodes, leaf, cam, "reference") for _ in range(args.steps)]
     v = statistics.median(x["value"] for x in vals)
     base = dict(vals[-1])
     base["value"] = v
     line = {"metric": "Mrays/s", "value": v, "unit": "Mrays/s", "impl": "reference",
             "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": statistics.median(x["seconds"] for x in vals) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded procedural scene)",
-            "config": {"workload": WORKLOAD, "res": [W_RES, H_RES], "spp": SPP, "depth": DEPTH,
-                       "note": "reference runs 1 sample per step (bounded CPU sample)"},
+            "data": DATA, "config": frame_config(len(mesh.triangles), world),
+            "reference_sample": "each step renders 1 of the frame's %d samples per ray "
+                                "(bounded CPU sample; the metric counts queries, so it is "
+                                "comparable across spp)" % SPP,
+            "reference_scene": {"source": "stored workload -> OBJ -> the reference's hp::KDTree "
+                                          "(loader + SAH builder)",
+                                "build_s": build_s, "triangles": int(len(mesh.triangles)),
+                                "nodes": int(len(nodes))},
             "cpu_baseline": base,
             "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+DATA = "synthetic (seeded procedural scene, value-noise textures)"
+
+
+def frame_config(triangles, world):
+    """The frame workload's config dict, printed identically by both arms."""
+    return {"workload": WORKLOAD, "res": [W_RES, H_RES], "supersample": 1, "spp": SPP,
+            "depth": DEPTH, "triangles": int(triangles),
+            "l2": "flushed between frames (512 MiB write)",
+            "parallelism": "replicas" if world > 1 else "single"}
+
+
+def serve_summary(line, cpu):
+    """The serving keys of the default line: pose / panorama latency, the
+    stream's Mrays/s and its roofline fraction, next to a CPU baseline."""
+    keys = ("rate_per_s", "duration_s", "requests", "completed", "unfinished",
+            "pose_512x512_4spp", "pano_2048x1024_64spp", "Mrays_per_s", "Msamples_per_s",
+            "roofline", "scene_triangles", "scene_build_s", "server", "policy")
+    out = {k: line[k] for k in keys if k in line}
+    out["cpu_baseline"] = cpu
+    return out
+
+
+def serve_cpu_baseline(scene_arrays, cam):
+    """The reference kernels on the host cores rendering one pose request of
+    the spheres scene (512 x 512, depth 6) at 1 of its 4 samples: the pose
+    latency a CPU host would give, scaled to 4 samples."""
+    import oracle as O
+    mesh, nodes, leaf = scene_arrays
+    cs = O.CpuScene(mesh, nodes, leaf)
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    _, _, counts = cs.refcl_render(cam, 512, 512, 1, 1, (0.05, 0.05, 0.05), 1, 6, 0, 1.0,
+                                   seed=3, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"pose_latency_ms": dt * 4 * 1e3, "value": counts[0] / dt / 1e6, "unit": "Mrays/s",
+            "cores": threads, "kind": "reference",
+            "sample": "one 512x512 pose request of the spheres scene at 1 of 4 spp "
+                      "(%d queries, %.2f s), latency scaled x4" % (int(counts[0]), dt)}
 
 
 def rotate(v, axis, ang):
@@ -280,20 +423,15 @@ def c3_jobs(seed=0x48505403):
     return jobs
 
 
-def run_batch(args):
+def batch_c3(world, rank):
     """C3: 32 jobs one by one through hpt_render (the plain per-job path)
     against the same jobs in one hpt_batch wavefront with the autotuned
     tuning. Accumulators are compared bit for bit (counter RNG + fixed-point
     sums), so the relMSE of both against the reference estimate is identical
-    by construction."""
-    import torch
+    by construction. Returns the result line on rank 0 (None elsewhere)."""
     import hptracing_b200 as H
-    from hptracing_b200 import build as hbuild
     from hptracing_b200 import shard
     from hptracing_b200 import scenes as S
-    rank, world, local = dist_setup(args.gpus)
-    hbuild.build()
-    torch.cuda.set_device(local)
     all_jobs = c3_jobs()
     # With N ranks each runs its share (longest job first onto the least
     # loaded rank); the 32 jobs are the fixed total work (strong scaling).
@@ -319,15 +457,19 @@ def run_batch(args):
     for sc, _, _, _ in built:
         sc.set_tuning(tune)
 
+    per_job = []
+
     def plain():
         q = ms = 0.0
         accs = []
+        per_job.clear()
         t = time.perf_counter()
         for sc, cam, p, _ in built:
             _, acc = sc.render(cam, p, want_accum=True)
             st = sc.stats()
             q += st["intersect_queries"]
             ms += st["ms_total"]
+            per_job.append((st["ms_total"], st["intersect_queries"]))
             accs.append(acc)
         return q, ms, time.perf_counter() - t, accs
 
@@ -354,11 +496,19 @@ def run_batch(args):
     ms_p, ms_b = allreduce_max(ms_p, world), allreduce_max(ms_b, world)
     wall_p, wall_b = allreduce_max(wall_p, world), allreduce_max(wall_b, world)
     same = allreduce_sum(0.0 if same else 1.0, world) == 0.0
+    build_s = allreduce_max(build_s, world)
+    for sc, _, _, _ in built:
+        sc.close()
     if rank != 0:
-        for sc, _, _, _ in built:
-            sc.close()
-        return
+        return None
     work = [j["res"] ** 2 * j["spp"] * j["depth"] for j in all_jobs]
+    # Bound on the batch's gain for this job mix (one rank): the batch
+    # cannot finish before its largest job does when that job runs at its
+    # plain speed (it fills the wavefront alone), nor process the total
+    # queries faster than the best plain rate any job reached.
+    t_max = max(m for m, _ in per_job)
+    best_rate = max(q / m for m, q in per_job if m > 0)
+    bound = sum(m for m, _ in per_job) / max(t_max, sum(q for _, q in per_job) / best_rate)
     line = {
         "metric": "Mrays/s batched vs plain (C3, 32 mixed jobs)", "mode": "batch",
         "value": q_b / ms_b / 1e3, "unit": "Mrays/s", "plain": q_p / ms_p / 1e3,
@@ -368,15 +518,47 @@ def run_batch(args):
         "e2e": {"batched": q_b / wall_b / 1e6, "plain": q_p / wall_p / 1e6, "unit": "Mrays/s"},
         "accumulators_bit_identical": same,
         "largest_job_share_of_work": max(work) / sum(work),
+        "amdahl_bound": bound if world == 1 else None,
+        "largest_job_share_of_plain_ms": t_max / sum(m for m, _ in per_job),
         "tuning": {"capacity": tune.capacity, "isect_block": tune.isect_block,
                    "isect_min_blocks": tune.isect_min_blocks, "refill": tune.refill_chunk,
                    "smem_nodes": tune.smem_nodes, "use_graph": tune.use_graph,
                    "trav_steps": tune.trav_steps},
         "jobs": all_jobs,
         "scene_build_s": build_s, "dtype": "f32", "data": "synthetic (seeded scene families)"}
-    print(json.dumps(line), flush=True)
-    for sc, _, _, _ in built:
-        sc.close()
+    return line
+
+
+def run_batch(args):
+    import torch
+    from hptracing_b200 import build as hbuild
+    rank, world, local = dist_setup(args.gpus)
+    hbuild.build()
+    torch.cuda.set_device(local)
+    line = batch_c3(world, rank)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+def serve_scenes(terrain_n=1024):
+    """The four resident scenes of the serving stream: box room, spheres,
+    terrain and a larger terrain (heightfield terrain_n and 1.33 x terrain_n
+    vertices per side). Returns (scenes, cameras, triangle counts, build s)."""
+    import hptracing_b200 as H
+    from hptracing_b200 import scenes as S
+    t0 = time.perf_counter()
+    specs = [(0, {}), (1, dict(seed=1)),
+             (2, dict(seed=2, heightfield_n=terrain_n)),
+             (2, dict(seed=3, heightfield_n=int(terrain_n * 1.33)))]
+    scenes, cams, tris = [], [], []
+    for cfg, kw in specs:
+        mesh = H.Mesh.generate(cfg, **kw)
+        nodes, leaf = H.build_kdtree(mesh.points, mesh.triangles)
+        scenes.append(H.Scene(mesh, nodes, leaf))
+        cams.append(S.terrain_cam(1.0) if cfg == 2 else S.ROOM_CAM)
+        tris.append(len(mesh.triangles))
+        del mesh, nodes, leaf
+    return scenes, cams, tris, time.perf_counter() - t0
 
 
 def run_serve(args):
@@ -391,30 +573,21 @@ def run_serve(args):
     from hptracing_b200 import scenes as S
     hbuild.build()
     torch.cuda.set_device(0)
-    t0 = time.perf_counter()
-    specs = [(0, {}), (1, dict(seed=1)),
-             (2, dict(seed=2, heightfield_n=args.terrain_n)),
-             (2, dict(seed=3, heightfield_n=int(args.terrain_n * 1.33)))]
-    scenes, cams, tris = [], [], []
-    for cfg, kw in specs:
-        mesh = H.Mesh.generate(cfg, **kw)
-        nodes, leaf = H.build_kdtree(mesh.points, mesh.triangles)
-        scenes.append(H.Scene(mesh, nodes, leaf))
-        cams.append(S.terrain_cam(1.0) if cfg == 2 else S.ROOM_CAM)
-        tris.append(len(mesh.triangles))
-        del mesh, nodes, leaf
-    build_s = time.perf_counter() - t0
+    scenes, cams, tris, build_s = serve_scenes(args.terrain_n)
     for rate in [float(x) for x in str(args.rate).split(",")]:
         for cap in [int(x) for x in str(args.serve_capacity).split(",")]:
             for pct in [int(x) for x in str(args.large_pct).split(",")]:
                 for ahead in [int(x) for x in str(args.depth_ahead).split(",")]:
-                    serve_stream(H, S, scenes, cams, tris, build_s, rate, args, cap, pct, ahead)
+                    line = serve_stream(H, S, scenes, cams, tris, build_s, rate, args.duration,
+                                        cap, pct, ahead)
+                    print(json.dumps(line), flush=True)
     for sc in scenes:
         sc.close()
 
 
-def serve_stream(H, S, scenes, cams, tris, build_s, rate, args, capacity, large_pct, ahead):
-    """One Poisson stream at `rate` requests/s against a fresh server."""
+def serve_stream(H, S, scenes, cams, tris, build_s, rate, duration, capacity, large_pct, ahead):
+    """One Poisson stream at `rate` requests/s for `duration` seconds
+    against a fresh server; returns the result line."""
     server = H.Server(max_jobs=64, memory_budget=16 << 30, capacity=capacity,
                       large_inflight_pct=large_pct, pipeline_depth=ahead, keep_accum=0)
     slots = [server.add_scene(s) for s in scenes]
@@ -422,7 +595,7 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, args, capacity, large_
     arrivals, t = [], 0.0
     while True:
         t += rng.exponential(1.0 / rate)
-        if t > args.duration:
+        if t > duration:
             break
         k = int(rng.integers(0, 4))
         if rng.random() < 0.8:
@@ -453,7 +626,7 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, args, capacity, large_
     pumps, gaps, last_pump_end = [], [], None
     samples = 0
     nxt = 0
-    drain_cap = args.duration + 20.0
+    drain_cap = duration + 20.0
     while True:
         now = time.perf_counter() - start
         while nxt < len(arrivals) and arrivals[nxt][0] <= now:
@@ -491,9 +664,19 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, args, capacity, large_
     def pct(v, x):
         return float(np.percentile(v, x)) if v else None
 
+    d = {k: st1[k] - st0[k] for k in ("intersect_queries", "shade_calls", "nodes_visited",
+                                        "leaves_visited", "triangle_tests")}
+    alg = (64 * d["intersect_queries"] + 72 * d["shade_calls"] + 8 * d["nodes_visited"] +
+           36 * d["leaves_visited"] + 48 * d["triangle_tests"])
+    peak, peak_kind = measured_peak()
     line = {
         "metric": "serving p50/p99 latency (C4)", "mode": "serve", "rate_per_s": rate,
-        "duration_s": args.duration, "elapsed_s": elapsed,
+        "duration_s": duration, "elapsed_s": elapsed,
+        "roofline": {"bound": "hbm", "kernel": "wavefront (traversal + queues), whole stream",
+                     "achieved": alg / elapsed / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / elapsed / 1e9 / peak, "peak_kind": peak_kind,
+                     "basis": "algorithmic bytes of every intersect query / the stream's wall "
+                              "time"},
         "requests": len(arrivals), "completed": len(lat["pose"]) + len(lat["pano"]),
         "unfinished": len(outstanding) + (len(arrivals) - nxt),
         "pose_512x512_4spp": {"n": len(lat["pose"]), "p50_ms": pct(lat["pose"], 50),
@@ -513,8 +696,8 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, args, capacity, large_
                    "pipeline_depth": ahead, "max_jobs": 64, "memory_budget": 16 << 30},
         "scene_triangles": tris, "scene_build_s": build_s, "clocks": clocks,
         "dtype": "f32", "data": "synthetic (seeded scenes, seeded Poisson stream)"}
-    print(json.dumps(line), flush=True)
     server.close()
+    return line
 
 
 def run_compact(args):
@@ -678,16 +861,13 @@ def main():
         obuild.build()
         kind = "reference" if O.refcl_lib() is not None else "port"
         base = cpu_baseline(mesh, nodes, leaf, cam, kind)
+    line = None
     if rank == 0:
         line = {
             "metric": "Mrays/s", "value": value, "unit": "Mrays/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded procedural scene, random textures)",
-            "config": {"workload": WORKLOAD, "res": [W_RES, H_RES], "supersample": 1,
-                       "spp": SPP, "depth": DEPTH, "triangles": int(len(mesh.triangles)),
-                       "l2": "flushed between frames (512 MiB write)",
-                       "parallelism": "replicas" if world > 1 else "single"},
+            "data": DATA, "config": frame_config(len(mesh.triangles), world),
             "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": 320,
                     "d2h_bytes_per_step": W_RES * H_RES * 4 + 256},
             "gpu_launches": launches,
@@ -716,8 +896,35 @@ def main():
             "clocks": clocks,
             "cpu_baseline": base,
         }
-        print(json.dumps(line), flush=True)
     scene.close()
+    del flush
+    torch.cuda.empty_cache()
+    if not args.frame_only and WORKLOAD.startswith("spheres64"):
+        # The metric's other two parts on the same box: the 32-job batch
+        # (batched vs one by one, bit-identical accumulators, hence equal
+        # relMSE) and the serving stream at 50 requests/s.
+        b = batch_c3(world, rank)
+        if rank == 0:
+            line["batch"] = {k: b[k] for k in (
+                "metric", "value", "plain", "speedup", "unit", "ms_batched", "ms_plain",
+                "queries", "e2e", "accumulators_bit_identical", "largest_job_share_of_work",
+                "largest_job_share_of_plain_ms", "amdahl_bound", "tuning", "scene_build_s",
+                "jobs_per_rank") if k in b}
+        if world == 1:
+            import hptracing_b200 as H
+            from hptracing_b200 import scenes as S
+            scenes, cams, tris, sbuild = serve_scenes()
+            sl = serve_stream(H, S, scenes, cams, tris, sbuild, 50.0, args.serve_seconds,
+                              1 << 20, 5, 1)
+            for sc in scenes:
+                sc.close()
+            cpu = None if args.no_cpu_baseline else serve_cpu_baseline((mesh, nodes, leaf), cam)
+            line["serve"] = serve_summary(sl, cpu)
+        elif rank == 0:
+            line["serve"] = {"skipped": "the serving stream runs at N = 1 (one server per "
+                                        "device; requests are routed, not split)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -779,7 +779,10 @@ static_assert(kNoallocMaxBlocks * kCompactTile == HPT_COMPACT_NOALLOC_MAX_N,
 static __device__ __align__(256) int g_noalloc_block_counts[kNoallocMaxBlocks + 1];
 
 // Device address of g_noalloc_block_counts, looked up once per device with
-// that device current (the first call on a device does this set-up).
+// that device current (the first call on a device does this set-up). The
+// cached address belongs to the device's current context: after a
+// cudaDeviceReset the caller must not use this entry point again in the
+// same process.
 hpt_status noalloc_scratch(int device, int** out) {
   static std::mutex mu;
   static std::vector<int*> addr;
@@ -807,7 +810,8 @@ extern "C" hpt_status hpt_compact_noalloc(const uint32_t* flags, int32_t n, int3
   int device = 0;
   HPT_CUDA(cudaGetDevice(&device));
   int* scratch = nullptr;
-  hpt_status s = noalloc_scratch(device, &scratch);
+  // The lookup table may grow (host memory): no exception leaves the ABI.
+  hpt_status s = guarded([&]() -> hpt_status { return noalloc_scratch(device, &scratch); });
   if (s != HPT_OK) return s;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (n == 0) {

@@ -11,18 +11,32 @@
 //  - removeEmptyNode folds an empty leaf child into its parent (:171-206);
 //  - getData: pre-order nodes, leaf list [count, ids...], sibling on left
 //    children only (:248-292).
-// Differences that do not change the output: the candidate list is a merge
-// of the two sorted arrays instead of a re-sort, min/max arrays are freed
-// after a node is split, and large subtrees are built on worker threads.
+// Differences that do not change the output:
+//  - a triangle's min / max along an axis does not depend on the node, so a
+//    child's sorted arrays are its parent's sorted (value, triangle) arrays
+//    filtered to the child's triangles (linear per node) instead of being
+//    recomputed and re-sorted (the reference sorts 6 arrays per node). The
+//    filtered arrays hold the same values in the same order; the one case
+//    where the order of equal values shows in the output (+0.0 and -0.0 in
+//    one candidate list, see best_split) recomputes that axis the
+//    reference's way, and so do small nodes (thread-local scratch);
+//  - the candidate list is a merge of the two sorted arrays instead of a
+//    re-sort;
+//  - nodes come from per-thread arenas, subtrees are built by a pool of
+//    worker threads, and the largest nodes scan their three axes in
+//    parallel; getData numbers nodes through an index kept in each node.
 #include <algorithm>
 #include <atomic>
 #include <cfloat>
+#include <climits>
 #include <cmath>
 #include <functional>
 #include <memory>
 #include <string>
 #include <thread>
-#include <unordered_map>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
 
 #include "host.h"
 
@@ -31,22 +45,131 @@ namespace hpt {
 namespace {
 
 struct Node {
-  std::unique_ptr<Node> left, right;
+  Node* left = nullptr;
+  Node* right = nullptr;
   Node* parent = nullptr;
   float box_start[3], box_end[3];
   std::vector<int32_t> geo;
+  int32_t index = -1;  // pre-order position (getData)
 };
+
+// Nodes come from per-thread arenas owned by the builder: no allocation per
+// node on the hot path and no per-node delete (tens of millions of nodes on
+// the large scenes); chunks grow geometrically.
+struct NodeArena {
+  std::vector<std::unique_ptr<Node[]>> chunks;
+  size_t used = 0, size = 0;
+  Node* make() {
+    if (used == size) {
+      size = size ? std::min<size_t>(2 * size, 1 << 16) : 256;
+      chunks.emplace_back(new Node[size]);
+      used = 0;
+    }
+    return &chunks.back()[used++];
+  }
+};
+
+// Sorted (value, triangle) arrays of a node: per axis, the triangles' minima
+// and maxima in ascending value order.
+struct Keyed {
+  float v;
+  int32_t id;
+};
+struct NodeLists {
+  std::vector<Keyed> mins[3], maxs[3];
+};
+
+// A child subtree of more than this many triangles is handed to the worker
+// pool when a worker is idle; smaller ones are built by the thread that
+// split their parent.
+constexpr size_t kTaskMin = 1024;
+// Nodes above this many triangles scan their three axes on three threads.
+constexpr size_t kParallelAxes = 1 << 15;
+// Nodes up to this many triangles sort their own values (in thread-local
+// scratch) instead of receiving filtered arrays from their parent.
+constexpr size_t kSmallNode = 256;
+
+std::atomic<uint64_t> g_builder_generation{0};
 
 struct Builder {
   const F4* points;
   const I4* tris;
-  std::atomic<int> threads_left{0};
+  int num_tris = 0;
+  const uint64_t generation = ++g_builder_generation;
+  std::mutex arenas_mu;
+  std::vector<std::unique_ptr<NodeArena>> arenas;
+  // Worker pool: subtrees waiting to be built, and how many are queued or
+  // being built (the build is done when none are).
+  struct Task {
+    Node* node;
+    NodeLists lists;
+  };
+  std::mutex q_mu;
+  std::condition_variable q_cv;
+  std::deque<Task> queue;
+  int outstanding = 0;
+  std::atomic<int> idle{0};
+
+  // This thread's arena for this build.
+  Node* make_node() {
+    thread_local uint64_t tl_generation = 0;
+    thread_local NodeArena* tl_arena = nullptr;
+    if (tl_generation != generation) {
+      std::lock_guard<std::mutex> lk(arenas_mu);
+      arenas.emplace_back(new NodeArena());
+      tl_arena = arenas.back().get();
+      tl_generation = generation;
+    }
+    return tl_arena->make();
+  }
+
+  // Builds the subtree of `n` here, or queues it for an idle worker.
+  void build_subtree(Node* n, NodeLists&& L) {
+    if (n->geo.size() > kTaskMin && idle.load(std::memory_order_relaxed) > 0) {
+      std::lock_guard<std::mutex> lk(q_mu);
+      queue.push_back(Task{n, std::move(L)});
+      ++outstanding;
+      q_cv.notify_one();
+      return;
+    }
+    split(n, std::move(L));
+  }
+
+  void worker() {
+    std::unique_lock<std::mutex> lk(q_mu);
+    while (true) {
+      idle.fetch_add(1);
+      q_cv.wait(lk, [&] { return !queue.empty() || outstanding == 0; });
+      idle.fetch_sub(1);
+      if (queue.empty()) return;  // nothing queued or running: done
+      Task t = std::move(queue.front());
+      queue.pop_front();
+      lk.unlock();
+      split(t.node, std::move(t.lists));
+      lk.lock();
+      if (--outstanding == 0) q_cv.notify_all();
+    }
+  }
+
+  void run(Node* root, NodeLists&& L, int threads) {
+    {
+      std::lock_guard<std::mutex> lk(q_mu);
+      queue.push_back(Task{root, std::move(L)});
+      outstanding = 1;
+    }
+    std::vector<std::thread> th;
+    for (int i = 1; i < threads; ++i) th.emplace_back([this] { worker(); });
+    worker();
+    for (std::thread& t : th) t.join();
+  }
 
   float coord(int vertex, int d) const {
     const F4& p = points[vertex];
     return d == 0 ? p.x : d == 1 ? p.y : p.z;
   }
 
+  // kdtree.cpp:23-34: the node's triangle minima and maxima along d, each
+  // sorted with std::sort from the node's triangle order.
   void min_max(const std::vector<int32_t>& geo, int d, std::vector<float>& mins,
                std::vector<float>& maxs) const {
     mins.resize(geo.size());
@@ -61,11 +184,58 @@ struct Builder {
     std::sort(maxs.begin(), maxs.end());
   }
 
+  // The root's sorted arrays: computed and sorted once.
+  void root_lists(const std::vector<int32_t>& geo, int d, NodeLists& L) const {
+    std::vector<Keyed>& mn = L.mins[d];
+    std::vector<Keyed>& mx = L.maxs[d];
+    mn.resize(geo.size());
+    mx.resize(geo.size());
+    for (size_t i = 0; i < geo.size(); ++i) {
+      const I4& t = tris[geo[i]];
+      float v[3] = {coord(t.x, d), coord(t.y, d), coord(t.z, d)};
+      mn[i] = {*std::min_element(v, v + 3), geo[i]};
+      mx[i] = {*std::max_element(v, v + 3), geo[i]};
+    }
+    auto by_value = [](const Keyed& a, const Keyed& b) { return a.v < b.v; };
+    std::sort(mn.begin(), mn.end(), by_value);
+    std::sort(mx.begin(), mx.end(), by_value);
+  }
+
+  static bool mixed_zeros(const std::vector<Keyed>& a, const std::vector<Keyed>& b) {
+    bool pos_zero = false, neg_zero = false;
+    for (const std::vector<Keyed>* v : {&a, &b})
+      for (const Keyed& k : *v)
+        if (k.v == 0.f) (std::signbit(k.v) ? neg_zero : pos_zero) = true;
+    return pos_zero && neg_zero;
+  }
+
+  // Best split along axis d (kdtree.cpp:47-89), from the node's filtered
+  // arrays when it has them (L != nullptr), else from its own sort.
+  void axis_split(const Node* node, const NodeLists* L, int d, float& best_pos,
+                  float& best_cost) const {
+    thread_local std::vector<float> mins, maxs;
+    if (!L || mixed_zeros(L->mins[d], L->maxs[d])) {
+      // The order of +0.0 and -0.0 among themselves is the reference's sort
+      // order of this node's own arrays: small nodes, and this rare case,
+      // compute them its way.
+      min_max(node->geo, d, mins, maxs);
+    } else {
+      const std::vector<Keyed>& mn = L->mins[d];
+      const std::vector<Keyed>& mx = L->maxs[d];
+      mins.resize(mn.size());
+      maxs.resize(mx.size());
+      for (size_t i = 0; i < mn.size(); ++i) mins[i] = mn[i].v;
+      for (size_t i = 0; i < mx.size(); ++i) maxs[i] = mx[i].v;
+    }
+    best_split(mins, maxs, node->box_start[d], node->box_end[d], best_pos, best_cost);
+  }
+
   // kdtree.cpp:47-89
   static void best_split(const std::vector<float>& mins,
                          const std::vector<float>& maxs, float box_start,
                          float box_end, float& best_pos, float& best_cost) {
-    std::vector<float> all(mins.size() + maxs.size());
+    thread_local std::vector<float> all;
+    all.resize(mins.size() + maxs.size());
     // +0.0 and -0.0 compare equal, so their order in the sorted candidate
     // list (and with it the bits of a chosen split at zero) is whatever the
     // reference's std::sort of the concatenation produces. Sort the same way
@@ -101,28 +271,32 @@ struct Builder {
     }
   }
 
-  // kdtree.cpp:93-169
-  void split(Node* node) {
-    if (node->geo.size() < 5) return;
-    float no_split_cost = 3.f * node->geo.size();
+  // kdtree.cpp:93-169. L: the node's filtered sorted arrays (consumed), or
+  // empty for a node of at most kSmallNode triangles.
+  void split(Node* node, NodeLists L) {
+    const size_t n = node->geo.size();
+    if (n < 5) return;
+    const NodeLists* lists = n > kSmallNode ? &L : nullptr;
+    float no_split_cost = 3.f * n;
     float best_pos[3], best_val[3];
-    {
-      std::vector<float> mins, maxs;
-      for (int d = 0; d < 3; ++d) {
-        min_max(node->geo, d, mins, maxs);
-        best_split(mins, maxs, node->box_start[d], node->box_end[d], best_pos[d],
-                   best_val[d]);
-      }
+    if (n > kParallelAxes) {
+      std::thread t1([&] { axis_split(node, lists, 1, best_pos[1], best_val[1]); });
+      std::thread t2([&] { axis_split(node, lists, 2, best_pos[2], best_val[2]); });
+      axis_split(node, lists, 0, best_pos[0], best_val[0]);
+      t1.join();
+      t2.join();
+    } else {
+      for (int d = 0; d < 3; ++d) axis_split(node, lists, d, best_pos[d], best_val[d]);
     }
     int bd = (int)(std::min_element(best_val, best_val + 3) - best_val);
     if (best_val[bd] > no_split_cost) return;
     float pos = best_pos[bd];
     if (pos <= node->box_start[bd] || pos >= node->box_end[bd]) return;
 
-    node->left.reset(new Node());
-    node->right.reset(new Node());
-    Node* l = node->left.get();
-    Node* r = node->right.get();
+    Node* l = make_node();
+    Node* r = make_node();
+    node->left = l;
+    node->right = r;
     l->parent = r->parent = node;
     for (int d = 0; d < 3; ++d) {
       l->box_start[d] = r->box_start[d] = node->box_start[d];
@@ -130,50 +304,70 @@ struct Builder {
     }
     l->box_end[bd] = pos;
     r->box_start[bd] = pos;
+    // Side of every triangle of the node (bit 0 left, bit 1 right), in this
+    // thread's own table (subtrees on other threads share triangles).
+    thread_local std::vector<uint8_t> side;
+    if ((int)side.size() < num_tris) side.assign(num_tris, 0);
+    size_t nl = 0, nr = 0;
     for (int32_t g : node->geo) {
       const I4& t = tris[g];
       float v[3] = {coord(t.x, bd), coord(t.y, bd), coord(t.z, bd)};
-      if (!(v[0] > pos && v[1] > pos && v[2] > pos)) l->geo.push_back(g);
-      if (!(v[0] < pos && v[1] < pos && v[2] < pos)) r->geo.push_back(g);
+      const bool to_l = !(v[0] > pos && v[1] > pos && v[2] > pos);
+      const bool to_r = !(v[0] < pos && v[1] < pos && v[2] < pos);
+      nl += to_l;
+      nr += to_r;
+      side[g] = (uint8_t)((to_l ? 1 : 0) | (to_r ? 2 : 0));
+    }
+    l->geo.resize(nl);
+    r->geo.resize(nr);
+    {
+      size_t il = 0, ir = 0;
+      for (int32_t g : node->geo) {
+        if (side[g] & 1) l->geo[il++] = g;
+        if (side[g] & 2) r->geo[ir++] = g;
+      }
     }
     std::vector<int32_t>().swap(node->geo);
-
-    // The two subtrees are independent; big ones go to a worker thread.
-    bool spawn = false;
-    if (l->geo.size() > 20000 && r->geo.size() > 20000) {
-      if (threads_left.fetch_sub(1) > 0)
-        spawn = true;
-      else
-        threads_left.fetch_add(1);
+    // The children's sorted arrays: the node's, filtered (order kept).
+    NodeLists LL, RL;
+    if (lists) {
+      const bool need_l = nl > kSmallNode, need_r = nr > kSmallNode;
+      for (int d = 0; d < 3; ++d) {
+        for (int m = 0; m < 2; ++m) {
+          std::vector<Keyed>& src = m ? L.maxs[d] : L.mins[d];
+          std::vector<Keyed>& dl = m ? LL.maxs[d] : LL.mins[d];
+          std::vector<Keyed>& dr = m ? RL.maxs[d] : RL.mins[d];
+          if (need_l) dl.reserve(nl);
+          if (need_r) dr.reserve(nr);
+          for (const Keyed& k : src) {
+            const uint8_t sd = side[k.id];
+            if (need_l && (sd & 1)) dl.push_back(k);
+            if (need_r && (sd & 2)) dr.push_back(k);
+          }
+          std::vector<Keyed>().swap(src);
+        }
+      }
     }
-    if (spawn) {
-      std::thread th([this, l] { split(l); });
-      split(r);
-      th.join();
-      threads_left.fetch_add(1);
-    } else {
-      split(l);
-      split(r);
-    }
+    // The two subtrees are independent.
+    build_subtree(r, std::move(RL));
+    build_subtree(l, std::move(LL));
   }
 
   // kdtree.cpp:171-206
   static void remove_empty(Node* n) {
     if (!n->left && !n->right) return;
-    remove_empty(n->left.get());
-    remove_empty(n->right.get());
-    Node* l = n->left.get();
-    Node* r = n->right.get();
+    remove_empty(n->left);
+    remove_empty(n->right);
+    Node* l = n->left;
+    Node* r = n->right;
     if (l && l->geo.empty() && !l->left && !l->right) {
       for (int d = 0; d < 3; ++d) {
         n->box_start[d] = r->box_start[d];
         n->box_end[d] = r->box_end[d];
       }
-      n->geo = r->geo;
-      std::unique_ptr<Node> rl = std::move(r->left);
-      std::unique_ptr<Node> rr = std::move(r->right);
-      n->left = std::move(rl);
-      n->right = std::move(rr);
+      n->geo = std::move(r->geo);
+      n->left = r->left;
+      n->right = r->right;
       if (n->right) n->right->parent = n;
       if (n->left) n->left->parent = n;
       return;
@@ -183,15 +377,27 @@ struct Builder {
         n->box_start[d] = l->box_start[d];
         n->box_end[d] = l->box_end[d];
       }
-      n->geo = l->geo;
-      std::unique_ptr<Node> lr = std::move(l->right);
-      std::unique_ptr<Node> ll = std::move(l->left);
-      n->right = std::move(lr);
-      n->left = std::move(ll);
+      n->geo = std::move(l->geo);
+      n->right = l->right;
+      n->left = l->left;
       if (n->right) n->right->parent = n;
       if (n->left) n->left->parent = n;
       return;
     }
+  }
+
+  // Releases every arena, several at a time.
+  void release() {
+    std::vector<std::unique_ptr<NodeArena>> all = std::move(arenas);
+    const size_t workers =
+        std::min<size_t>(all.size(), std::max(1u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    std::atomic<size_t> next{0};
+    for (size_t w = 0; w < workers; ++w)
+      th.emplace_back([&] {
+        for (size_t i = next++; i < all.size(); i = next++) all[i].reset();
+      });
+    for (std::thread& t : th) t.join();
   }
 };
 
@@ -217,69 +423,86 @@ hpt_status build_kdtree(const F4* points, int num_points, const I4* tris,
   Builder b;
   b.points = points;
   b.tris = tris;
+  b.num_tris = num_tris;
   if (num_threads <= 0) num_threads = (int)std::max(1u, std::thread::hardware_concurrency());
-  b.threads_left = num_threads - 1;
 
-  std::unique_ptr<Node> root(new Node());
+  Node* root = b.make_node();
   root->geo.resize(num_tris);
   for (int i = 0; i < num_tris; ++i) root->geo[i] = i;
-  {  // setBoxSize on the root only (kdtree.cpp:36-41, 235-246)
-    std::vector<float> mins, maxs;
-    for (int d = 0; d < 3; ++d) {
-      b.min_max(root->geo, d, mins, maxs);
-      root->box_start[d] = mins.front() - 1e-3f;
-      root->box_end[d] = maxs.back() + 1e-3f;
-    }
+  // setBoxSize on the root only (kdtree.cpp:36-41, 235-246): the smallest
+  // minimum and largest maximum per axis, +- 1e-3. The sorted arrays hold
+  // exactly those values at their ends.
+  NodeLists lists;
+  {
+    std::thread t1([&] { b.root_lists(root->geo, 1, lists); });
+    std::thread t2([&] { b.root_lists(root->geo, 2, lists); });
+    b.root_lists(root->geo, 0, lists);
+    t1.join();
+    t2.join();
   }
-  b.split(root.get());
-  Builder::remove_empty(root.get());
+  for (int d = 0; d < 3; ++d) {
+    root->box_start[d] = lists.mins[d].front().v - 1e-3f;
+    root->box_end[d] = lists.maxs[d].back().v + 1e-3f;
+  }
+  if ((size_t)num_tris <= kSmallNode) lists = NodeLists();
+  b.run(root, std::move(lists), num_threads);
+  Builder::remove_empty(root);
 
-  // getData (kdtree.cpp:248-292): pre-order numbering.
+  // getData (kdtree.cpp:248-292): pre-order numbering, left subtree first.
   std::vector<Node*> order;
-  std::vector<Node*> stack{root.get()};
-  while (!stack.empty()) {
-    Node* n = stack.back();
-    stack.pop_back();
-    order.push_back(n);
-    if (n->right) stack.push_back(n->right.get());
-    if (n->left) stack.push_back(n->left.get());
+  {
+    std::vector<Node*> stack{root};
+    while (!stack.empty()) {
+      Node* n = stack.back();
+      stack.pop_back();
+      n->index = (int32_t)order.size();
+      order.push_back(n);
+      if (n->right) stack.push_back(n->right);
+      if (n->left) stack.push_back(n->left);
+    }
   }
-  std::unordered_map<const Node*, int> index;
-  index.reserve(order.size() * 2);
-  for (size_t i = 0; i < order.size(); ++i) index[order[i]] = (int)i;
-
+  // Leaf list offsets in pre-order, then the nodes and lists filled in
+  // parallel.
+  std::vector<int64_t> offset(order.size() + 1, 0);
+  for (size_t i = 0; i < order.size(); ++i)
+    offset[i + 1] = offset[i] + (order[i]->geo.empty() ? 0 : 1 + (int64_t)order[i]->geo.size());
+  if (offset.back() > INT32_MAX) {
+    b.release();
+    return fail(HPT_ERR_OUT_OF_MEMORY, "kdtree: leaf list too long");
+  }
   out.nodes.assign(order.size(), hpt_ref_node());
-  out.leaf_data.clear();
-  for (size_t i = 0; i < order.size(); ++i) {
-    Node* n = order[i];
-    hpt_ref_node& h = out.nodes[i];
-    h.data = -1;
-    if (!n->geo.empty()) {
-      h.data = (int32_t)out.leaf_data.size();
-      out.leaf_data.push_back((int32_t)n->geo.size());
-      out.leaf_data.insert(out.leaf_data.end(), n->geo.begin(), n->geo.end());
-    }
-    for (int d = 0; d < 3; ++d) {
-      h.box_start[d] = n->box_start[d];
-      h.box_end[d] = n->box_end[d];
-    }
-    h.box_start[3] = h.box_end[3] = 0.f;
-    h.child = n->left ? index[n->left.get()] : -1;
-    h.parent = n->parent ? index[n->parent] : -1;
-    h.sibling = -1;
-    if (n->parent && n->parent->right && n->parent->right.get() != n)
-      h.sibling = index[n->parent->right.get()];
+  out.leaf_data.assign((size_t)offset.back(), 0);
+  {
+    const size_t workers = (size_t)std::max(1, num_threads);
+    std::vector<std::thread> th;
+    const size_t per = (order.size() + workers - 1) / workers;
+    for (size_t w = 0; w < workers; ++w)
+      th.emplace_back([&, w] {
+        const size_t lo = w * per, hi = std::min(order.size(), lo + per);
+        for (size_t i = lo; i < hi; ++i) {
+          const Node* n = order[i];
+          hpt_ref_node& h = out.nodes[i];
+          h.data = -1;
+          if (!n->geo.empty()) {
+            h.data = (int32_t)offset[i];
+            out.leaf_data[offset[i]] = (int32_t)n->geo.size();
+            std::copy(n->geo.begin(), n->geo.end(), out.leaf_data.begin() + offset[i] + 1);
+          }
+          for (int d = 0; d < 3; ++d) {
+            h.box_start[d] = n->box_start[d];
+            h.box_end[d] = n->box_end[d];
+          }
+          h.box_start[3] = h.box_end[3] = 0.f;
+          h.child = n->left ? n->left->index : -1;
+          h.parent = n->parent ? n->parent->index : -1;
+          h.sibling = -1;
+          if (n->parent && n->parent->right && n->parent->right != n)
+            h.sibling = n->parent->right->index;
+        }
+      });
+    for (std::thread& t : th) t.join();
   }
-  // Free the pointer tree iteratively (deep trees would overflow the stack
-  // through recursive unique_ptr destructors).
-  std::vector<std::unique_ptr<Node>> kill;
-  kill.push_back(std::move(root));
-  while (!kill.empty()) {
-    std::unique_ptr<Node> n = std::move(kill.back());
-    kill.pop_back();
-    if (n->left) kill.push_back(std::move(n->left));
-    if (n->right) kill.push_back(std::move(n->right));
-  }
+  b.release();
   return HPT_OK;
 }
 

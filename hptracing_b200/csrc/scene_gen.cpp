@@ -15,8 +15,11 @@
 // reader produces, so no emissive triangle has its right angle at v0 (the
 // reference's light-area formula divides by the cosine at v0).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 #include "host.h"
 
@@ -65,6 +68,21 @@ struct ValueNoise {
     return (float)sum;
   }
 };
+
+// Runs f(row) for rows [0, n) on all host cores.
+template <typename F>
+void parallel_rows(int n, F&& f) {
+  const int workers = (int)std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()),
+                                              (unsigned)std::max(1, n));
+  std::atomic<int> next{0};
+  std::vector<std::thread> th;
+  auto run = [&] {
+    for (int r = next++; r < n; r = next++) f(r);
+  };
+  for (int w = 1; w < workers; ++w) th.emplace_back(run);
+  run();
+  for (std::thread& t : th) t.join();
+}
 
 struct V3 {
   double x, y, z;
@@ -199,7 +217,8 @@ struct Builder {
     m.texture_data.resize(off + (size_t)size * size * 4);
     uint8_t* dst = m.texture_data.data() + off;
     float c0[3] = {(float)((seed >> 3) % 7) / 7.f, 0.5f, 0.9f};
-    for (int y = 0; y < size; ++y)
+    // Every texel is a pure function of (x, y): rows are filled in parallel.
+    parallel_rows(size, [&](int y) {
       for (int x = 0; x < size; ++x) {
         double u = 16.0 * x / size, v = 16.0 * y / size;
         float a = 0.5f + n.fbm(u, v, 4), b = 0.5f + n2.fbm(u * 2, v * 2, 3);
@@ -210,6 +229,7 @@ struct Builder {
         }
         px[3] = 0;
       }
+    });
     m.texture_names.push_back("noise" + std::to_string(m.texture_names.size()));
   }
 };
@@ -272,14 +292,23 @@ void terrain(Builder& b, Rng& rng, int n, int tex_size, int ntex,
   auto height = [&](double x, double z) { return 0.15 * noise.fbm(x * 2.5 + 7, z * 2.5 + 3, 6); };
   int base = (int)b.m.points.size();
   double h = 2.0 / (n - 1);
-  for (int i = 0; i < n; ++i)
+  // Heights and normals are pure functions of the grid point: computed in
+  // parallel by rows, appended in row order.
+  std::vector<V3> pos((size_t)n * n), nrm((size_t)n * n);
+  parallel_rows(n, [&](int i) {
     for (int j = 0; j < n; ++j) {
       double x = -1 + j * h, z = -1 + i * h;
       double y = height(x, z);
       double dx = (height(x + h, z) - height(x - h, z)) / (2 * h);
       double dz = (height(x, z + h) - height(x, z - h)) / (2 * h);
-      V3 nrm = normalized(V3{-dx, 1, -dz});
-      b.vertex(V3{x, y, z}, nrm, (x + 1) * 2, (z + 1) * 2);
+      pos[(size_t)i * n + j] = V3{x, y, z};
+      nrm[(size_t)i * n + j] = normalized(V3{-dx, 1, -dz});
+    }
+  });
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      const V3& p = pos[(size_t)i * n + j];
+      b.vertex(p, nrm[(size_t)i * n + j], (p.x + 1) * 2, (p.z + 1) * 2);
     }
   for (int i = 0; i + 1 < n; ++i)
     for (int j = 0; j + 1 < n; ++j) {

@@ -355,7 +355,9 @@ hpt_status hpt_compact(const uint32_t* flags, int32_t n, int32_t* out,
  * any stream capture. Every call shares the one array: calls whose work
  * overlaps on the GPU (different streams, or host threads) race on it and
  * must be serialised by the caller. Each call overwrites every scratch
- * entry it reads, so no state carries over between calls. */
+ * entry it reads, so no state carries over between calls. The array's
+ * address is cached per device: after cudaDeviceReset this entry point
+ * must not be called again in the same process. */
 #define HPT_COMPACT_NOALLOC_MAX_N (16384 * 2048)
 hpt_status hpt_compact_noalloc(const uint32_t* flags, int32_t n,
                                int32_t* out, int32_t* count, void* stream);

@@ -1,5 +1,8 @@
 """Writes a Mesh as Wavefront OBJ + MTL (geometry and materials, no texture
-maps) so the same scene can be read by the reference's own loader."""
+maps) so the same scene can be read by the reference's own loader
+(checker infrastructure: the oracle pins and bench.py's reference arm).
+`mesh` is anything with the hp::Scene arrays: points, normals, texcoords,
+triangles (v0, v1, v2, material) and materials (the 96-byte records)."""
 import os
 
 import numpy as np

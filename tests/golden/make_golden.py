@@ -46,7 +46,7 @@ sys.path.insert(0, ROOT)
 import hptracing_b200 as H  # noqa: E402
 import oracle as O  # noqa: E402
 from tests import scenes as S  # noqa: E402
-from tests import objio  # noqa: E402
+from oracle import objio  # noqa: E402
 
 from oracle import build as obuild  # noqa: E402
 

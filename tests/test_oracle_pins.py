@@ -18,7 +18,7 @@ import pytest
 import hptracing_b200 as H
 import oracle as O
 from oracle import build as obuild
-from tests import objio
+from oracle import objio
 from tests import scenes as S
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
