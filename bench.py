@@ -61,6 +61,8 @@ def parse():
     # Overrides for profiling runs only (the headline workload is the default).
     ap.add_argument("--res", type=int, default=0)
     ap.add_argument("--spp", type=int, default=0)
+    ap.add_argument("--tuning", default="",
+                    help="frame: hpt_tuning fields to override, e.g. shade_min_blocks=3")
     # Extra workloads (one JSON line each): the 32-job mixed batch, batched
     # vs one job at a time; the Poisson serving stream.
     ap.add_argument("--mode", default="frame", choices=["frame", "batch", "serve", "compact"])
@@ -815,6 +817,9 @@ def main():
     camera = S.hp_camera(cam)
     tune = scene.tuning()
     tune.profile = 1
+    for kv in filter(None, args.tuning.split(",")):
+        k, v = kv.split("=")
+        setattr(tune, k, int(v))
     scene.set_tuning(tune)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
 
@@ -894,6 +899,7 @@ def main():
                           "tri_tests_per_query": stats[-1]["triangle_tests"] / stats[-1][
                               "intersect_queries"]},
             "clocks": clocks,
+            "tuning": {f: getattr(tune, f) for f, _ in type(tune)._fields_},
             "cpu_baseline": base,
         }
     scene.close()

@@ -115,7 +115,9 @@ class Mesh:
 
     @classmethod
     def load_obj(cls, filename, mtl_basepath="", texture_size=512, ignore_textures=False):
-        """hp::Scene::Scene (src/hp/scene/base.cpp:37-158)."""
+        """hp::Scene::Scene (src/hp/scene/base.cpp:37-158). texture_size > 0
+        resamples every texture to that square size (512: the reference's
+        behaviour); 0 keeps each texture at its own size (texture_dims)."""
         h = C.c_void_p()
         check(lib().hpt_mesh_load_obj(filename.encode(), mtl_basepath.encode(),
                                       texture_size, int(ignore_textures), C.byref(h)))

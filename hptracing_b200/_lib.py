@@ -94,7 +94,7 @@ class Tuning(C.Structure):
     _fields_ = [("capacity", i32), ("isect_block", i32), ("shade_block", i32),
                 ("refill_chunk", i32), ("smem_nodes", i32), ("use_graph", i32),
                 ("profile", i32), ("isect_min_blocks", i32), ("trav_steps", i32),
-                ("max_steps", i32)]
+                ("max_steps", i32), ("shade_min_blocks", i32)]
 
 
 class ServerConfig(C.Structure):

@@ -73,7 +73,9 @@ int usage() {
           "usage: hptracing -i scene.obj|generated:K -o out.ppm [--mtl DIR] [--width W]\n"
           "       [--height H] [--view x,y,z] [--up x,y,z] [--right x,y,z] [--angle A]\n"
           "       [-x] [-s SAMPLES] [-d DEPTH] [--brightness B] [--no-diffuse]\n"
-          "       [--background r,g,b] [--seed N] [--device D] [--keys SEQ]\n");
+          "       [--background r,g,b] [--seed N] [--device D] [--keys SEQ]\n"
+          "       [--texture-size N]   (N > 0: every texture resized to N x N, as the\n"
+          "                             reference does with 512; 0: native sizes)\n");
   return 2;
 }
 
@@ -172,7 +174,7 @@ std::string frame_name(const std::string& out, int k) {
 
 int main(int argc, char** argv) {
   std::string input, mtl, output, keys;
-  int width = 500, height = 500, sample = 10, depth = 6, device = 0;
+  int width = 500, height = 500, sample = 10, depth = 6, device = 0, texture_size = 512;
   float angle = 1.0f, brightness = 1.0f;
   bool supersample = false, no_diffuse = false;
   uint64_t seed = 0;
@@ -205,6 +207,7 @@ int main(int argc, char** argv) {
     else if (a == "--seed") seed = strtoull(next(), nullptr, 10);
     else if (a == "--device") device = atoi(next());
     else if (a == "--keys") keys = next();
+    else if (a == "--texture-size") texture_size = atoi(next());
     else return usage();
   }
   if (input.empty() || output.empty()) return usage();
@@ -218,7 +221,7 @@ int main(int argc, char** argv) {
       size_t pos = input.rfind('/');
       if (pos != std::string::npos && pos > 0) mtl = input.substr(0, pos + 1);
     }
-    st = hpt_mesh_load_obj(input.c_str(), mtl.c_str(), 512, 0, &mesh);
+    st = hpt_mesh_load_obj(input.c_str(), mtl.c_str(), texture_size, 0, &mesh);
   }
   if (st != HPT_OK) {
     fprintf(stderr, "hptracing: %s: %s\n", hpt_status_string(st), hpt_last_error());
@@ -235,11 +238,8 @@ int main(int argc, char** argv) {
   copy_view(scene.materials, v.materials, v.num_materials);
   scene.texture_data.assign(v.texture_data, v.texture_data + v.texture_bytes);
   scene.texture_names.resize(v.num_textures);
-  int tex_w = 512, tex_h = 512;
-  if (v.num_textures > 0) {
-    tex_w = v.texture_dims[0];
-    tex_h = v.texture_dims[1];
-  }
+  if (v.num_textures > 0)
+    scene.texture_dims.assign(v.texture_dims, v.texture_dims + 2 * (size_t)v.num_textures);
   hpt_kdtree* tree = nullptr;
   st = hpt_kdtree_build(v.points, v.num_points, v.triangles, v.num_triangles, 0, &tree);
   if (st != HPT_OK) {
@@ -258,7 +258,7 @@ int main(int argc, char** argv) {
   std::vector<unsigned char> pixels((size_t)width * height * 4);
   try {
     Scene* sp = &scene;
-    hp::TraceRunner runner(sp, device, tex_w, tex_h);
+    hp::TraceRunner runner(sp, device);
     float step = 1.f;  // translate_step, hptracing.cpp:58
     int frame = 0;
     auto render = [&](const std::string& path) -> bool {

@@ -412,7 +412,8 @@ hpt_status check_tuning(const hpt_tuning& t) {
   if (t.capacity < 1024 || t.capacity > (1 << 27) || t.smem_nodes < 0 ||
       t.smem_nodes > kMaxSmemNodes || t.refill_chunk < 1 || t.refill_chunk > 32 ||
       (t.isect_block != 128 && t.isect_block != 256) || t.isect_min_blocks < 0 ||
-      t.trav_steps < 0 || t.trav_steps > 256 || t.max_steps < 0)
+      t.trav_steps < 0 || t.trav_steps > 256 || t.max_steps < 0 ||
+      (t.shade_min_blocks != 0 && t.shade_min_blocks != 3 && t.shade_min_blocks != 4))
     return fail(HPT_ERR_INVALID_ARGUMENT, "tuning out of range");
   return HPT_OK;
 }

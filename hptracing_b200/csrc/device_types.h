@@ -130,14 +130,17 @@ struct DevCtrl {
   int32_t nA;               // paths in the current shade queue
   int32_t nR;               // rays in the intersect queue
   int32_t nA_next;          // hits appended by the intersect kernel
-  int32_t isect_head;       // refill cursor of the intersect kernel
-  int32_t prim_head;        // refill cursor of the primary kernel
   int32_t parity;           // which shade buffer is current
   int32_t n_new;            // new paths granted to the coming shade pass
   int32_t done;             // no queued path and nothing left to issue
   int32_t n_quota;          // slots with a grant (quota_slot / quota_prefix)
   int32_t n_order;          // slots in priority order (host-written)
   int64_t iterations;
+  // Refill cursors of the intersect and primary kernels. 64-bit: one
+  // admission's primary rays may exceed 2^31 (several jobs of up to 2^30
+  // rays each).
+  unsigned long long isect_head;
+  unsigned long long prim_head;
   DevErr err;
   unsigned long long isect_queries;
   unsigned long long shades;

@@ -250,12 +250,16 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
   int slot = 0;
   int64_t ray = 0;
   uint32_t queries = 0;  // this lane's queries in this launch
+  // Once a refill finds the rays exhausted the warp stops asking (the value
+  // is warp-uniform), so the cursor overshoots by at most one grab per warp.
+  bool drained = false;
   while (true) {
     const unsigned idle = __ballot_sync(kFull, !active);
-    if (__popc(idle) >= P.refill) {
-      int base = 0;
-      if (lane == 0) base = atomicAdd(&c->prim_head, __popc(idle));
+    if (!drained && __popc(idle) >= P.refill) {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(&c->prim_head, (unsigned long long)__popc(idle));
       base = __shfl_sync(kFull, base, 0);
+      drained = (int64_t)base + __popc(idle) >= total;
       if (!active) {
         const int64_t g = (int64_t)base + __popc(idle & lanemask_lt());
         if (g < total) {
@@ -351,8 +355,12 @@ __global__ void k_admit(EngineParams P) {
 // ---------------------------------------------------------------------------
 // Shade + next direction (+ new paths), compacting survivors into R.
 // ---------------------------------------------------------------------------
-template <int BS>
-__global__ void __launch_bounds__(BS) k_shade(EngineParams P) {
+// MINB: blocks of BS threads per SM the register budget must fit (1 leaves
+// the compiler's natural allocation, ~106 registers = 2 blocks of 256). The
+// kernel is bound by gather latency, so resident warps can pay for a few
+// spills; the tuning chooses.
+template <int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) k_shade(EngineParams P) {
   __shared__ int warp_counts[BS / 32];
   __shared__ int block_base;
   DevCtrl* c = P.ctrl;
@@ -520,20 +528,23 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
   int item = 0;   // index in the intersect queue; the payload is reloaded at the end
   int slot = 0;
   uint32_t queries = 0;  // this lane's queries in this launch
+  // As in k_primary: a warp that finds the queue exhausted stops refilling.
+  bool drained = false;
   while (true) {
     const unsigned idle = __ballot_sync(kFull, !active);
-    if (__popc(idle) >= P.refill) {
-      int base = 0;
-      if (lane == 0) base = atomicAdd(&c->isect_head, __popc(idle));
+    if (!drained && __popc(idle) >= P.refill) {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(&c->isect_head, (unsigned long long)__popc(idle));
       base = __shfl_sync(kFull, base, 0);
+      drained = (int64_t)base + __popc(idle) >= n;
       if (!active) {
-        const int i = base + __popc(idle & lanemask_lt());
+        const int64_t i = (int64_t)base + __popc(idle & lanemask_lt());
         if (i < n) {
           bool ok = true;
           HPT_DCHECK(&c->err, i < P.capacity, 221, i, ok = false);
           if (ok) {
             const float4 o4 = P.R_o[i], d4 = P.R_d[i];
-            item = i;
+            item = (int)i;
             slot = __float_as_int(P.R_s[i].w);
             HPT_DCHECK(&c->err, slot >= 0 && slot < P.num_slots, 222, slot, ok = false);
             if (ok) {
@@ -669,6 +680,14 @@ const IsectVariant kIsectVariants[] = {
 };
 #undef HPT_ISECT_VARIANT
 constexpr int kNumIsectVariants = sizeof(kIsectVariants) / sizeof(kIsectVariants[0]);
+
+// The shading kernel for a tuning's register budget (shade_min_blocks 3 or
+// 4 blocks of 256 per SM; anything else: the natural allocation).
+void (*shade_kernel(const hpt_tuning& t))(EngineParams) {
+  if (t.shade_min_blocks == 3) return k_shade<256, 3>;
+  if (t.shade_min_blocks == 4) return k_shade<256, 4>;
+  return k_shade<256, 1>;
+}
 
 __device__ __forceinline__ float ray_value(const unsigned long long* acc, const uint32_t* flags,
                                            int64_t ray, int ch) {
@@ -997,7 +1016,7 @@ hpt_status Engine::query_occupancy() {
   HPT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &b, v.isect_kernel(tuning.trav_steps, tuning.smem_nodes), v.block, smem));
   occ_isect_ = std::max(1, b);
-  HPT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<256>, 256, 0));
+  HPT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, shade_kernel(tuning), 256, 0));
   occ_shade_ = std::max(1, b);
   occ_done_ = true;
   return HPT_OK;
@@ -1287,7 +1306,8 @@ hpt_status Engine::ensure_graph(const DevScene* shared_scene, int iterations) {
   if (graph_exec_ && same_scene && graph_capacity_ == capacity_ &&
       graph_slots_ == slots_ && graph_iters_ == iterations && graph_tuning_ == isect_variant() &&
       graph_smem_ == tuning.smem_nodes && graph_refill_ == tuning.refill_chunk &&
-      graph_steps_ == tuning.trav_steps && graph_max_steps_ == tuning.max_steps)
+      graph_steps_ == tuning.trav_steps && graph_max_steps_ == tuning.max_steps &&
+      graph_shade_ == tuning.shade_min_blocks)
     return HPT_OK;
   if (graph_exec_) {
     HPT_SOFT(cudaGraphExecDestroy(graph_exec_));
@@ -1316,6 +1336,7 @@ hpt_status Engine::ensure_graph(const DevScene* shared_scene, int iterations) {
   graph_refill_ = tuning.refill_chunk;
   graph_steps_ = tuning.trav_steps;
   graph_max_steps_ = tuning.max_steps;
+  graph_shade_ = tuning.shade_min_blocks;
   return HPT_OK;
 }
 
@@ -1326,7 +1347,7 @@ void Engine::launch_iteration(const DevScene* shared_scene, cudaEvent_t* ev) {
                                quota_prefix_, prim_slot_, prim_prefix_, 0, capacity_, A, A_tri_,
                                A_leaf_, R, shared_scene);
   if (ev) HPT_SOFT(cudaEventRecord(ev[0], stream));
-  k_shade<256><<<num_sms * occ_shade_, 256, 0, stream>>>(P);
+  shade_kernel(tuning)<<<num_sms * occ_shade_, 256, 0, stream>>>(P);
   if (ev) HPT_SOFT(cudaEventRecord(ev[1], stream));
   const size_t smem = (size_t)P.smem_nodes * sizeof(uint2);
   const IsectVariant& v = kIsectVariants[isect_variant()];

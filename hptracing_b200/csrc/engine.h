@@ -158,6 +158,7 @@ class Engine {
   DevScene graph_scene_{};
   int graph_capacity_ = 0, graph_slots_ = 0, graph_iters_ = 0, graph_tuning_ = -1;
   int graph_smem_ = -1, graph_refill_ = -1, graph_steps_ = -1, graph_max_steps_ = -1;
+  int graph_shade_ = -1;
   hpt_status init_status_ = HPT_OK;
   hpt_status init();
   int occ_isect_ = 1, occ_shade_ = 1;

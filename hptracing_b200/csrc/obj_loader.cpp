@@ -441,7 +441,9 @@ hpt_status load_obj(const std::string& filename, const std::string& basepath,
     material_probabilities(x);
     out.materials.push_back(x);
   }
-  if (texture_size <= 0) texture_size = 512;  // base.cpp:34-35
+  // base.cpp:31-32 resizes every texture to 512 x 512; texture_size > 0 does
+  // the same at that size, 0 keeps each texture at its own size.
+  if (texture_size < 0) return fail(HPT_ERR_INVALID_ARGUMENT, "texture_size must be >= 0");
   for (const std::string& name : out.texture_names) {  // base.cpp:98-110
     int w = 0, h = 0;
     std::vector<float> rgb;
@@ -456,16 +458,18 @@ hpt_status load_obj(const std::string& filename, const std::string& basepath,
       out.texture_data.insert(out.texture_data.end(), grey, grey + 4);
       continue;
     }
-    // normalize(0, 255) then nearest resample to texture_size^2, RGB + 0.
+    // normalize(0, 255) then nearest resample to tw x th, RGB + 0.
     float lo = *std::min_element(rgb.begin(), rgb.end());
     float hi = *std::max_element(rgb.begin(), rgb.end());
     float scale = hi > lo ? 255.f / (hi - lo) : 0.f;
-    out.texture_dims.push_back(texture_size);
-    out.texture_dims.push_back(texture_size);
-    for (int i = 0; i < texture_size; ++i) {
-      int sy = (int)((int64_t)i * h / texture_size);
-      for (int j = 0; j < texture_size; ++j) {
-        int sx = (int)((int64_t)j * w / texture_size);
+    const int tw = texture_size > 0 ? texture_size : w;
+    const int th = texture_size > 0 ? texture_size : h;
+    out.texture_dims.push_back(tw);
+    out.texture_dims.push_back(th);
+    for (int i = 0; i < th; ++i) {
+      int sy = (int)((int64_t)i * h / th);
+      for (int j = 0; j < tw; ++j) {
+        int sx = (int)((int64_t)j * w / tw);
         for (int k = 0; k < 3; ++k)
           out.texture_data.push_back((uint8_t)((rgb[((size_t)sy * w + sx) * 3 + k] - lo) * scale));
         out.texture_data.push_back(0);

@@ -621,6 +621,7 @@ bool cache_lookup(const char* path, const std::string& key, hpt_tuning* t) {
     if (!(is >> k >> x.capacity >> x.isect_block >> x.isect_min_blocks >> x.refill_chunk >>
           x.smem_nodes >> x.use_graph >> x.trav_steps))
       continue;
+    if (!(is >> x.shade_min_blocks)) x.shade_min_blocks = default_tuning().shade_min_blocks;
     if (k == key) {
       *t = x;
       return true;
@@ -634,7 +635,7 @@ void cache_store(const char* path, const std::string& key, const hpt_tuning& t) 
   std::ofstream f(path, std::ios::app);
   f << key << " " << t.capacity << " " << t.isect_block << " " << t.isect_min_blocks << " "
     << t.refill_chunk << " " << t.smem_nodes << " " << t.use_graph << " " << t.trav_steps
-    << "\n";
+    << " " << t.shade_min_blocks << "\n";
 }
 
 }  // namespace
@@ -702,6 +703,7 @@ extern "C" hpt_status hpt_autotune(hpt_scene* scene, const hpt_camera* camera,
       {{{1 << 20, 0}, {1 << 21, 0}, {1 << 22, 0}},
        [](hpt_tuning& t, int a, int) { t.capacity = a; }},
       {{{0, 0}, {1, 0}}, [](hpt_tuning& t, int a, int) { t.use_graph = a; }},
+      {{{0, 0}, {3, 0}, {4, 0}}, [](hpt_tuning& t, int a, int) { t.shade_min_blocks = a; }},
   };
   for (const Knob& k : knobs) {
     for (const auto& v : k.values) {

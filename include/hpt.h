@@ -115,10 +115,12 @@ typedef struct hpt_mesh_arrays {
  * (src/hp/scene/base.cpp:37-158, parser semantics of the vendored
  * tinyobjloader src/objloader/tiny_obj_loader.cpp:278-723), including the
  * material branch probabilities and the 256-entry light table.
- * Textures: binary/ASCII PPM (P6/P3) are decoded and resampled
- * (nearest) to texture_size x texture_size; other formats return
- * HPT_ERR_UNSUPPORTED unless ignore_textures != 0, in which case every
- * texture becomes a 1x1 mid-grey layer. */
+ * Textures: binary/ASCII PPM (P6/P3) are decoded; texture_size > 0
+ * resamples (nearest) every texture to texture_size x texture_size (512
+ * is the reference's behaviour, base.cpp:31-32, 101-102), 0 keeps each
+ * texture at its own size (hpt_mesh_arrays.texture_dims lists them).
+ * Other formats return HPT_ERR_UNSUPPORTED unless ignore_textures != 0,
+ * in which case every texture becomes a 1x1 mid-grey layer. */
 hpt_status hpt_mesh_load_obj(const char* filename, const char* mtl_basepath,
                              int32_t texture_size, int32_t ignore_textures,
                              hpt_mesh** out);
@@ -281,6 +283,9 @@ typedef struct hpt_tuning {
                              /* HPT_ERR_TRAVERSAL_LIMIT; 0 = the scene's  */
                              /* cap, 8 x (nodes + leaf references) +      */
                              /* 100000. Larger values are clamped to it.  */
+  int32_t shade_min_blocks;  /* register budget of the shading kernel:    */
+                             /* 3 or 4 blocks of 256 threads per SM; 0 =  */
+                             /* the natural allocation (2 blocks)         */
 } hpt_tuning;
 hpt_status hpt_tuning_get(const hpt_scene* scene, hpt_tuning* out);
 hpt_status hpt_tuning_set(hpt_scene* scene, const hpt_tuning* in);

@@ -22,6 +22,8 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "hpt.h"
@@ -40,6 +42,53 @@ inline void check(hpt_status s, const char* where) {
   if (s != HPT_OK) throw Error(s, where);
 }
 
+namespace detail {
+template <class...>
+struct voider {
+  using type = void;
+};
+// The reference's hp::Scene resizes every texture to its static
+// texture_width x texture_height (src/hp/scene/base.h:28, base.cpp:31-32).
+template <class S, class = void>
+struct has_layer_size : std::false_type {};
+template <class S>
+struct has_layer_size<S, typename voider<decltype(S::texture_width),
+                                         decltype(S::texture_height)>::type> : std::true_type {};
+// A scene that keeps its textures at their own sizes lists (w, h) per
+// texture in texture_dims.
+template <class S, class = void>
+struct has_texture_dims : std::false_type {};
+template <class S>
+struct has_texture_dims<S, typename voider<decltype(std::declval<S&>().texture_dims)>::type>
+    : std::true_type {};
+
+// Tags: (has_layer_size, has_texture_dims).
+template <class S, class D>
+void layer_dims(const S&, int ntex, int w, int h, std::vector<int32_t>& dims,
+                std::true_type /*static size*/, D) {
+  dims.assign(2 * (size_t)ntex, 0);
+  for (int t = 0; t < ntex; ++t) {
+    dims[2 * t] = w > 0 ? w : (int)S::texture_width;
+    dims[2 * t + 1] = h > 0 ? h : (int)S::texture_height;
+  }
+}
+template <class S>
+void layer_dims(const S& s, int ntex, int, int, std::vector<int32_t>& dims, std::false_type,
+                std::true_type /*texture_dims*/) {
+  dims.assign(s.texture_dims.begin(), s.texture_dims.end());
+  dims.resize(2 * (size_t)ntex, 0);
+}
+template <class S>
+void layer_dims(const S&, int ntex, int w, int h, std::vector<int32_t>& dims, std::false_type,
+                std::false_type) {
+  dims.assign(2 * (size_t)ntex, 0);
+  for (int t = 0; t < ntex; ++t) {
+    dims[2 * t] = w > 0 ? w : 512;
+    dims[2 * t + 1] = h > 0 ? h : 512;
+  }
+}
+}  // namespace detail
+
 }  // namespace hpt
 
 namespace hp {
@@ -47,23 +96,27 @@ namespace hp {
 class TraceRunner {
  public:
   // TraceRunner(std::unique_ptr<hp::KDTree> & scene), trace_runner.h:51.
-  // texture_width/height: the per-layer size of scene->texture_data (the
-  // reference resizes every texture to Scene::texture_width x height).
+  // The size of each texture layer in scene->texture_data comes from the
+  // scene type: the reference's static Scene::texture_width x
+  // texture_height (every texture resized to it), or a per-texture
+  // `texture_dims` list (w, h, ...) where the scene keeps native sizes.
+  // texture_width/height > 0 override the static size; a scene type with
+  // neither member uses them, or 512 x 512 (the reference's size).
   template <class ScenePtr>
-  explicit TraceRunner(ScenePtr& scene, int device = 0, int texture_width = 512,
-                       int texture_height = 512) {
+  explicit TraceRunner(ScenePtr& scene, int device = 0, int texture_width = 0,
+                       int texture_height = 0) {
     auto data = scene->getData();
     const auto& nodes = data.first;
     const auto& leaf = data.second;
     static_assert(sizeof(nodes[0]) == sizeof(hpt_ref_node), "KDTreeNodeHeader is 48 bytes");
     static_assert(sizeof(scene->materials[0]) == sizeof(hpt_ref_material),
                   "Material is 96 bytes");
+    using S = typename std::remove_cv<typename std::remove_reference<decltype(*scene)>::type>::type;
     const int ntex = (int)scene->texture_names.size();
-    std::vector<int32_t> dims(2 * (size_t)ntex);
-    for (int t = 0; t < ntex; ++t) {
-      dims[2 * t] = texture_width;
-      dims[2 * t + 1] = texture_height;
-    }
+    std::vector<int32_t> dims;
+    hpt::detail::layer_dims(*scene, ntex, texture_width, texture_height, dims,
+                            hpt::detail::has_layer_size<S>(),
+                            hpt::detail::has_texture_dims<S>());
     hpt_scene_desc d;
     std::memset(&d, 0, sizeof d);
     d.points = reinterpret_cast<const float*>(scene->points.data());

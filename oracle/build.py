@@ -16,6 +16,10 @@
        (src/hp/scene/*.cpp, src/hp/common.cpp, src/objloader/*.cpp) compiled
        with refshim/Eigen/Core and refshim/CL/cl.h, driven by
        refscene_driver.cpp.
+     - dropin_runner: dropin_main.cpp, the C++ drop-in header
+       include/hpt_trace_runner.hpp used with the reference's own hp::KDTree
+       and cl_float3 (the same scene sources and stand-ins), linked against
+       hptracing_b200/libhpt.so (when that is built).
    Nothing is compiled with the reference's own build system and no
    reference source is copied into the repository.
 """
@@ -30,6 +34,8 @@ REF_OUT = os.path.join(HERE, "_ref")
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 REFCL_LIB = os.path.join(REF_OUT, "librefcl.so")
 REFSCENE_LIB = os.path.join(REF_OUT, "librefscene.so")
+DROPIN_BIN = os.path.join(REF_OUT, "dropin_runner")
+REPO = os.path.dirname(HERE)
 FLAGS = ["-O2", "-std=c++14", "-fPIC", "-shared", "-pthread", "-ffp-contract=off"]
 
 
@@ -100,7 +106,29 @@ def build_reference():
                                 "-include", "map", "-include", "algorithm",
                                 "-include", "functional", "-include", "cstring"]
              + srcs + ["-o", REFSCENE_LIB])
+    build_dropin(root, srcs[:-1], shims)
     return REFCL_LIB
+
+
+def build_dropin(root, scene_srcs, shims):
+    """The drop-in checker: the reference's scene sources + dropin_main.cpp,
+    linked against libhpt.so (found at run time next to the repository,
+    $ORIGIN/../../hptracing_b200)."""
+    lib = os.path.join(REPO, "hptracing_b200", "libhpt.so")
+    main = os.path.join(HERE, "dropin_main.cpp")
+    hdrs = [os.path.join(REPO, "include", "hpt_trace_runner.hpp"),
+            os.path.join(REPO, "include", "hpt.h")]
+    if not (os.path.exists(lib) and all(os.path.exists(s) for s in scene_srcs)):
+        return None
+    if _stale(DROPIN_BIN, scene_srcs + shims + hdrs + [main, lib]):
+        _run(["g++", "-O2", "-std=c++14", "-pthread", "-ffp-contract=off", "-w",
+              "-I", os.path.join(HERE, "refshim"), "-I", os.path.join(root, "src"),
+              "-I", os.path.join(REPO, "include"),
+              "-include", "map", "-include", "algorithm", "-include", "functional",
+              "-include", "cstring"] + scene_srcs + [main, "-o", DROPIN_BIN,
+                                                      "-L", os.path.dirname(lib), "-lhpt",
+                                                      "-Wl,-rpath,$ORIGIN/../../hptracing_b200"])
+    return DROPIN_BIN
 
 
 def build():
@@ -111,5 +139,5 @@ def build():
 if __name__ == "__main__":
     build()
     print(ORACLE_LIB)
-    for p in (REFCL_LIB, REFSCENE_LIB):
+    for p in (REFCL_LIB, REFSCENE_LIB, DROPIN_BIN):
         print(p, os.path.exists(p))

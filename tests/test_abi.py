@@ -122,3 +122,45 @@ def test_cli_builds_and_parses_flags(built):
     assert os.access(cli, os.X_OK)
     r = subprocess.run([cli, "--bogus"], capture_output=True, text=True)
     assert r.returncode == 2 and "usage" in r.stderr
+
+
+def _write_textured_obj(d):
+    """Two triangles, each with a PPM texture of its own size."""
+    def ppm(name, w, h, seed):
+        rng = np.random.default_rng(seed)
+        px = rng.integers(0, 256, (h, w, 3), dtype=np.uint8)
+        with open(os.path.join(d, name), "wb") as f:
+            f.write(b"P6\n%d %d\n255\n" % (w, h) + px.tobytes())
+        return px
+    a = ppm("a.ppm", 3, 5, 1)
+    b = ppm("b.ppm", 8, 2, 2)
+    with open(os.path.join(d, "t.mtl"), "w") as f:
+        f.write("newmtl ma\nKd 1 1 1\nmap_Kd a.ppm\n\nnewmtl mb\nKd 1 1 1\nmap_Kd b.ppm\n")
+    with open(os.path.join(d, "t.obj"), "w") as f:
+        f.write("mtllib t.mtl\nv 0 0 0\nv 1 0 0\nv 0 1 0\nv 1 1 0\nvt 0 0\nvt 1 0\nvt 0 1\n"
+                "vt 1 1\nusemtl ma\nf 1/1 2/2 3/3\nusemtl mb\nf 2/2 4/4 3/3\n")
+    return os.path.join(d, "t.obj"), a, b
+
+
+def _normalized(px):
+    """CImg normalize(0, 255) of one texture, as the loader applies it."""
+    lo, hi = px.min(), px.max()
+    return ((px.astype(np.float32) - lo) * np.float32(255.0 / (hi - lo))).astype(np.uint8)
+
+
+def test_loader_keeps_per_texture_sizes(built, tmp_path):
+    """texture_size 0 keeps each texture at its own size; a positive size
+    resamples all of them to it (512: the reference's behaviour)."""
+    path, a, b = _write_textured_obj(str(tmp_path))
+    m = H.Mesh.load_obj(path, str(tmp_path) + "/", texture_size=0)
+    assert m.texture_dims.tolist() == [[3, 5], [8, 2]]
+    data = np.asarray(m.texture_data, np.uint8)
+    la = data[:3 * 5 * 4].reshape(5, 3, 4)
+    lb = data[3 * 5 * 4:].reshape(2, 8, 4)
+    assert np.array_equal(la[:, :, :3], _normalized(a)) and (la[:, :, 3] == 0).all()
+    assert np.array_equal(lb[:, :, :3], _normalized(b)) and (lb[:, :, 3] == 0).all()
+    m4 = H.Mesh.load_obj(path, str(tmp_path) + "/", texture_size=4)
+    assert m4.texture_dims.tolist() == [[4, 4], [4, 4]]
+    assert len(m4.texture_data) == 2 * 4 * 4 * 4
+    with pytest.raises(H.HptError):
+        H.Mesh.load_obj(path, str(tmp_path) + "/", texture_size=-1)
