@@ -80,6 +80,8 @@ def parse():
                          "%% (comma list)")
     ap.add_argument("--depth-ahead", default="1",
                     help="serve: iterations queued ahead of the host (comma list)")
+    ap.add_argument("--deadline-ms", default="0",
+                    help="serve: overload policy deadline (0 = off; comma list)")
     ap.add_argument("--terrain-n", type=int, default=1024,
                     help="serve: heightfield vertices per side of the large scenes")
     return ap.parse_args()
@@ -580,18 +582,21 @@ def run_serve(args):
         for cap in [int(x) for x in str(args.serve_capacity).split(",")]:
             for pct in [int(x) for x in str(args.large_pct).split(",")]:
                 for ahead in [int(x) for x in str(args.depth_ahead).split(",")]:
-                    line = serve_stream(H, S, scenes, cams, tris, build_s, rate, args.duration,
-                                        cap, pct, ahead)
-                    print(json.dumps(line), flush=True)
+                    for dl in [int(x) for x in str(args.deadline_ms).split(",")]:
+                        line = serve_stream(H, S, scenes, cams, tris, build_s, rate,
+                                            args.duration, cap, pct, ahead, dl)
+                        print(json.dumps(line), flush=True)
     for sc in scenes:
         sc.close()
 
 
-def serve_stream(H, S, scenes, cams, tris, build_s, rate, duration, capacity, large_pct, ahead):
+def serve_stream(H, S, scenes, cams, tris, build_s, rate, duration, capacity, large_pct, ahead,
+                 deadline_ms=0):
     """One Poisson stream at `rate` requests/s for `duration` seconds
     against a fresh server; returns the result line."""
     server = H.Server(max_jobs=64, memory_budget=16 << 30, capacity=capacity,
-                      large_inflight_pct=large_pct, pipeline_depth=ahead, keep_accum=0)
+                      large_inflight_pct=large_pct, pipeline_depth=ahead, keep_accum=0,
+                      deadline_ms=deadline_ms)
     slots = [server.add_scene(s) for s in scenes]
     rng = np.random.default_rng(0x48505404 + int(rate))
     arrivals, t = [], 0.0
@@ -624,6 +629,7 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, duration, capacity, la
     start = time.perf_counter()
     outstanding = {}
     lat = {"pose": [], "pano": []}
+    shed = {"pose": 0, "pano": 0}
     per_scene = {}
     pumps, gaps, last_pump_end = [], [], None
     samples = 0
@@ -648,7 +654,13 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, duration, capacity, la
             last_pump_end = time.perf_counter()
             pumps.append(((tp - start) * 1e3, (last_pump_end - tp) * 1e3))
             for rid in server.completed():
-                st, info = server.poll(rid)
+                try:
+                    st, info = server.poll(rid)
+                except H.HptError as e:
+                    if e.status == 8 and rid in outstanding:  # shed by the overload policy
+                        shed[outstanding.pop(rid)[0]] += 1
+                        continue
+                    raise
                 if st == 0 and rid in outstanding:
                     kind, p, k = outstanding.pop(rid)
                     lat[kind].append(info["done_ms"] - info["submit_ms"])
@@ -680,6 +692,12 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, duration, capacity, la
                      "basis": "algorithmic bytes of every intersect query / the stream's wall "
                               "time"},
         "requests": len(arrivals), "completed": len(lat["pose"]) + len(lat["pano"]),
+        "shed": shed,
+        "policy": {"deadline_ms": deadline_ms,
+                   "rule": ("requests of <= capacity paths first-come first-served ahead of "
+                            "larger ones, admitted while the admitted ones are expected to "
+                            "finish within the deadline, shed when still queued past it")
+                   if deadline_ms > 0 else "smallest remaining work first, no shedding"},
         "unfinished": len(outstanding) + (len(arrivals) - nxt),
         "pose_512x512_4spp": {"n": len(lat["pose"]), "p50_ms": pct(lat["pose"], 50),
                               "p99_ms": pct(lat["pose"], 99)},

@@ -439,9 +439,10 @@ class Server:
     """Continuous-batching render server (hpt_server)."""
 
     def __init__(self, device=0, max_jobs=64, memory_budget=8 << 30, capacity=1 << 22,
-                 progressive=0, large_inflight_pct=0, pipeline_depth=0, keep_accum=1):
+                 progressive=0, large_inflight_pct=0, pipeline_depth=0, keep_accum=1,
+                 deadline_ms=0):
         cfg = ServerConfig(device, max_jobs, memory_budget, capacity, progressive,
-                           large_inflight_pct, pipeline_depth, keep_accum)
+                           large_inflight_pct, pipeline_depth, keep_accum, deadline_ms)
         h = C.c_void_p()
         check(lib().hpt_server_create(C.byref(cfg), C.byref(h)))
         self._h = h
@@ -458,6 +459,10 @@ class Server:
         check(lib().hpt_server_submit(self._h, slot, C.byref(camera), C.byref(params),
                                       C.byref(rid)))
         return rid.value
+
+    def shed(self):
+        """Requests shed by the overload policy so far."""
+        return lib().hpt_server_shed(self._h)
 
     def pump(self, max_iterations=1):
         check(lib().hpt_server_pump(self._h, max_iterations))

@@ -100,7 +100,7 @@ class Tuning(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("device", i32), ("max_jobs", i32), ("memory_budget", i64), ("capacity", i32),
                 ("progressive", i32), ("large_inflight_pct", i32), ("pipeline_depth", i32),
-                ("keep_accum", i32), ("reserved", i32 * 1)]
+                ("keep_accum", i32), ("deadline_ms", i32)]
 
 
 class RequestInfo(C.Structure):
@@ -151,6 +151,7 @@ SIGNATURES = {
     "hpt_server_poll": (i32, [vp, u64, P(RequestInfo), vp, vp]),
     "hpt_server_cancel": (i32, [vp, u64]),
     "hpt_server_pending": (i32, [vp]),
+    "hpt_server_shed": (i64, [vp]),
     "hpt_server_stats_get": (i32, [vp, P(RenderStats)]),
     "hpt_server_drain_completed": (i32, [vp, vp, i32, P(i32)]),
     "hpt_server_destroy": (None, [vp]),

@@ -160,87 +160,126 @@ __global__ void k_stage_resolve(const float* accum, int W, int H, int ssx, int s
   out[3] = 0;
 }
 
-// --- Stream compaction: warp ballot + block scan, three passes. ---------
+// --- Stream compaction: per-tile counts, one scan, stable scatter. -------
+// A tile is 2048 flags: 256 threads x 8 consecutive flags, read as two
+// 16-byte loads where the flag array is 16-byte aligned and the tile is
+// whole. No kernel waits on another block: the three passes are ordered by
+// the stream alone.
 constexpr int kCompactThreads = 256;
 constexpr int kCompactItems = 8;
 constexpr int kCompactTile = kCompactThreads * kCompactItems;
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 16;
 
-__device__ __forceinline__ unsigned lane_lt() {
-  unsigned m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+// This thread's 8 flags as a bit mask (bit k: flag i0 + k nonzero).
+__device__ __forceinline__ uint32_t load_flags8(const uint32_t* flags, int64_t i0, int n,
+                                                bool vec) {
+  uint32_t m = 0;
+  if (vec && i0 + kCompactItems <= n) {
+    const uint4 a = __ldg(reinterpret_cast<const uint4*>(flags + i0));
+    const uint4 b = __ldg(reinterpret_cast<const uint4*>(flags + i0) + 1);
+    m = (a.x != 0) | (a.y != 0) << 1 | (a.z != 0) << 2 | (a.w != 0) << 3 | (b.x != 0) << 4 |
+        (b.y != 0) << 5 | (b.z != 0) << 6 | (b.w != 0) << 7;
+  } else {
+    for (int k = 0; k < kCompactItems; ++k)
+      if (i0 + k < n && __ldg(flags + i0 + k) != 0) m |= 1u << k;
+  }
   return m;
 }
 
-__global__ void k_compact_count(const uint32_t* flags, int n, int* block_counts) {
-  __shared__ int warp_sum[kCompactThreads / 32];
-  const int64_t tile = (int64_t)blockIdx.x * kCompactTile;
-  int cnt = 0;
-  for (int k = 0; k < kCompactItems; ++k) {
-    const int64_t i = tile + (int64_t)k * kCompactThreads + threadIdx.x;
-    const bool f = i < n && flags[i] != 0;
-    cnt += __popc(__ballot_sync(0xFFFFFFFFu, f));
+// Exclusive scan of one value per thread over a block of BS threads;
+// *total receives the block's sum. Two barriers.
+template <int BS>
+__device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
+  __shared__ int warp_tot[BS / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int inc = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+    if (lane >= o) inc += y;
   }
-  if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = cnt;
+  if (lane == 31) warp_tot[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    int t = lane < BS / 32 ? warp_tot[lane] : 0;
+    int ti = t;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xFFFFFFFFu, ti, o);
+      if (lane >= o) ti += y;
+    }
+    if (lane < BS / 32) warp_tot[lane] = ti - t;  // exclusive warp offsets
+    const int all = __shfl_sync(0xFFFFFFFFu, ti, 31);
+    if (lane == 0) *total = all;
+  }
+  __syncthreads();
+  return warp_tot[warp] + inc - v;
+}
+
+__global__ void __launch_bounds__(kCompactThreads) k_compact_count(const uint32_t* flags, int n,
+                                                                   int* block_counts) {
+  __shared__ int warp_sum[kCompactThreads / 32];
+  const bool vec = (reinterpret_cast<uintptr_t>(flags) & 15) == 0;
+  const int64_t i0 = (int64_t)blockIdx.x * kCompactTile + (int64_t)threadIdx.x * kCompactItems;
+  const int c = __popc(load_flags8(flags, i0, n, vec));
+  const int w = __reduce_add_sync(0xFFFFFFFFu, c);
+  if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = w;
   __syncthreads();
   if (threadIdx.x == 0) {
-    int s = 0;
-    for (int w = 0; w < kCompactThreads / 32; ++w) s += warp_sum[w];
-    block_counts[blockIdx.x] = s;
+    int sum = 0;
+    for (int k = 0; k < kCompactThreads / 32; ++k) sum += warp_sum[k];
+    block_counts[blockIdx.x] = sum;
   }
 }
 
-// Exclusive scan of the block counts in place (one block, chunked).
-__global__ void k_compact_scan(int* counts, int nb, int* total) {
-  __shared__ int buf[1024];
-  __shared__ int carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
-  for (int base = 0; base < nb; base += 1024) {
-    const int i = base + threadIdx.x;
-    const int v = i < nb ? counts[i] : 0;
-    buf[threadIdx.x] = v;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-      const int add = threadIdx.x >= off ? buf[threadIdx.x - off] : 0;
-      __syncthreads();
-      buf[threadIdx.x] += add;
-      __syncthreads();
+// Exclusive scan of the tile counts in place (one block; 16 consecutive
+// counts per thread per chunk of 16,384), total to *total.
+__global__ void __launch_bounds__(kScanThreads) k_compact_scan(int* counts, int nb, int* total) {
+  __shared__ int chunk_total;
+  int carry = 0;
+  for (int base = 0; base < nb; base += kScanThreads * kScanItems) {
+    const int j0 = base + threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      v[k] = j0 + k < nb ? counts[j0 + k] : 0;
+      sum += v[k];
     }
-    if (i < nb) counts[i] = carry + buf[threadIdx.x] - v;
-    __syncthreads();
-    if (threadIdx.x == 1023) carry += buf[1023];
-    __syncthreads();
+    int tot = 0;
+    int off = block_exclusive_scan<kScanThreads>(sum, &chunk_total);
+    tot = chunk_total;
+    off += carry;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      if (j0 + k < nb) counts[j0 + k] = off;
+      off += v[k];
+    }
+    carry += tot;
+    __syncthreads();  // chunk_total is rewritten by the next chunk
   }
   if (threadIdx.x == 0) *total = carry;
 }
 
-__global__ void k_compact_scatter(const uint32_t* flags, int n, const int* block_offsets,
-                                  int* out) {
-  __shared__ int warp_base[kCompactThreads / 32];
-  __shared__ int running;
+__global__ void __launch_bounds__(kCompactThreads) k_compact_scatter(const uint32_t* flags, int n,
+                                                                     const int* block_offsets,
+                                                                     int* out) {
+  __shared__ int staged[kCompactTile];
+  __shared__ int tile_count;
+  const bool vec = (reinterpret_cast<uintptr_t>(flags) & 15) == 0;
   const int64_t tile = (int64_t)blockIdx.x * kCompactTile;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x == 0) running = block_offsets[blockIdx.x];
-  __syncthreads();
-  for (int k = 0; k < kCompactItems; ++k) {
-    const int64_t i = tile + (int64_t)k * kCompactThreads + threadIdx.x;
-    const bool f = i < n && flags[i] != 0;
-    const unsigned m = __ballot_sync(0xFFFFFFFFu, f);
-    if (lane == 0) warp_base[warp] = __popc(m);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int s = running;
-      for (int w = 0; w < kCompactThreads / 32; ++w) {
-        const int c = warp_base[w];
-        warp_base[w] = s;
-        s += c;
-      }
-      running = s;
-    }
-    __syncthreads();
-    if (f) out[warp_base[warp] + __popc(m & lane_lt())] = (int)i;
-    __syncthreads();
+  const int64_t i0 = tile + (int64_t)threadIdx.x * kCompactItems;
+  uint32_t m = load_flags8(flags, i0, n, vec);
+  int pos = block_exclusive_scan<kCompactThreads>(__popc(m), &tile_count);
+  // Survivor indices of the tile in order, staged in shared memory ...
+  while (m) {
+    const int k = __ffs(m) - 1;
+    m &= m - 1;
+    staged[pos++] = (int)(i0 + k);
   }
+  __syncthreads();
+  // ... then written out with consecutive threads on consecutive slots.
+  const int base = block_offsets[blockIdx.x];
+  for (int k = threadIdx.x; k < tile_count; k += kCompactThreads) out[base + k] = staged[k];
 }
 
 inline int blocks_for(int64_t n, int bs) { return (int)((n + bs - 1) / bs); }
@@ -315,12 +354,15 @@ hpt_status upload_scene(const hpt_scene_desc& d, SceneDev& out) {
   const DevTri* recs;
   const int32_t* refs;
   if ((s = dev_upload(out, pk.nodes.data(), pk.nodes.size(), &nodes)) != HPT_OK) return s;
+  const DevWide* wide;
+  if ((s = dev_upload(out, pk.wide.data(), pk.wide.size(), &wide)) != HPT_OK) return s;
   if ((s = dev_upload(out, pk.leaves.data(), pk.leaves.size(), &leaves)) != HPT_OK) return s;
   // At least one entry so the pointer is valid even for an empty tree.
   if (pk.refs.empty()) pk.refs.push_back(0);
   if ((s = dev_upload(out, pk.refs.data(), pk.refs.size(), &refs)) != HPT_OK) return s;
   if ((s = dev_upload(out, pk.tris.data(), pk.tris.size(), &recs)) != HPT_OK) return s;
   ds.nodes = nodes;
+  ds.wide = wide;
   ds.leaves = leaves;
   ds.leaf_refs = refs;
   ds.tris = recs;

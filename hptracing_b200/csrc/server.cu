@@ -59,6 +59,9 @@ enum RequestState { kQueued = 0, kRunning = 1, kDone = 2, kFailed = 3, kCancelle
 struct Request {
   uint64_t id = 0;
   JobSpec js;
+  int scene_slot = 0;
+  bool small = true;        // rays x spp <= capacity: latency-bound
+  bool shed = false;        // dropped by the overload policy
   int state = kQueued;
   int slot = -1;
   bool want_accum = true;
@@ -113,6 +116,13 @@ struct hpt_server {
   std::vector<cudaEvent_t> event_pool;
   int64_t completed = 0;
   int64_t pumps = 0;
+  // Overload policy (cfg.deadline_ms > 0): per-scene service time of a
+  // latency-bound request (its completion minus the later of its admission
+  // and the previous latency-bound completion, i.e. its time at the head of
+  // the first-come first-served line), smoothed; -1 = not measured yet.
+  std::vector<double> svc_ms;
+  double last_small_done_ms = 0;
+  int64_t shed = 0;
 
   double now_ms() const {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
@@ -127,20 +137,43 @@ struct hpt_server {
       if (slot_req[k] && !reqs.at(slot_req[k])->finishing) return true;
     return false;
   }
-  // Slots still computing, smallest remaining work first.
+  // Slots still computing in grant order: smallest remaining work first;
+  // under the overload policy, latency-bound requests first-come
+  // first-served ahead of all larger ones.
   std::vector<int> order() const {
-    std::vector<std::pair<int64_t, int>> v;
+    std::vector<std::pair<std::pair<int64_t, int64_t>, int>> v;
     for (size_t k = 0; k < slot_req.size(); ++k) {
       if (!slot_req[k]) continue;
       const Request* r = reqs.at(slot_req[k]).get();
       if (r->finishing) continue;
       const int64_t total = r->paths >= 0 ? r->paths : r->rays * r->js.params.sample;
-      v.push_back({total - r->done_paths, (int)k});
+      if (cfg.deadline_ms > 0)
+        v.push_back({{r->small ? 0 : 1, r->small ? (int64_t)r->id : total - r->done_paths},
+                     (int)k});
+      else
+        v.push_back({{0, total - r->done_paths}, (int)k});
     }
     std::stable_sort(v.begin(), v.end());
     std::vector<int> o;
     for (auto& p : v) o.push_back(p.second);
     return o;
+  }
+  double service_estimate(int scene) const {
+    return scene < (int)svc_ms.size() ? svc_ms[scene] : -1.0;
+  }
+  // Expected time until the latency-bound requests already admitted finish.
+  double small_backlog_ms() const {
+    double ms = 0;
+    for (size_t k = 0; k < slot_req.size(); ++k) {
+      if (!slot_req[k]) continue;
+      const Request* r = reqs.at(slot_req[k]).get();
+      if (!r->small || r->finishing) continue;
+      const double svc = service_estimate(r->scene_slot);
+      if (svc < 0) continue;
+      const double left = r->paths > 0 ? 1.0 - (double)r->done_paths / (double)r->paths : 1.0;
+      ms += svc * std::max(0.0, left);
+    }
+    return ms;
   }
   hpt_status take_pinned(size_t bytes, void** out) {
     auto it = pinned_pool.find(bytes);
@@ -176,6 +209,9 @@ hpt_status hpt_server::admit_pending() {
   std::vector<int> ids;
   std::vector<DevJob> jobs;
   std::vector<int64_t> rays;
+  const double now = now_ms();
+  double backlog = cfg.deadline_ms > 0 ? small_backlog_ms() : 0.0;
+  bool small_waiting = false;
   for (auto it = queue.begin(); it != queue.end();) {
     Request* r = find(*it);
     if (!r || r->cancel) {
@@ -185,6 +221,27 @@ hpt_status hpt_server::admit_pending() {
       }
       it = queue.erase(it);
       continue;
+    }
+    if (cfg.deadline_ms > 0 && r->small) {
+      // Overload policy: shed what can no longer meet its deadline; admit
+      // first-come first-served only while the admitted latency-bound work
+      // plus this request is expected to finish in time.
+      const double waited = now - r->submit_ms;
+      if (waited > cfg.deadline_ms) {
+        r->state = kCancelled;
+        r->shed = true;
+        ++shed;
+        finished_ids.push_back(r->id);
+        it = queue.erase(it);
+        continue;
+      }
+      const double svc = service_estimate(r->scene_slot);
+      if (small_waiting || (svc >= 0 && waited + backlog + svc > cfg.deadline_ms)) {
+        small_waiting = true;  // later latency-bound requests wait behind it
+        ++it;
+        continue;
+      }
+      if (svc >= 0) backlog += svc;
     }
     int slot = -1;
     for (size_t k = 0; k < slot_req.size(); ++k)
@@ -302,6 +359,14 @@ hpt_status hpt_server::retire_finished() {
     r->done_ms = now_ms();
     finished_ids.push_back(r->id);
     ++completed;
+    if (r->small && !r->cancel) {
+      const double head = std::max(r->admit_ms, last_small_done_ms);
+      const double dt = r->done_ms - head;
+      last_small_done_ms = r->done_ms;
+      if ((int)svc_ms.size() <= r->scene_slot) svc_ms.resize(r->scene_slot + 1, -1.0);
+      double& e = svc_ms[r->scene_slot];
+      e = e < 0 ? dt : 0.7 * e + 0.3 * dt;
+    }
   }
   return HPT_OK;
 }
@@ -379,12 +444,14 @@ hpt_status hpt_server_submit(hpt_server* server, int32_t scene_slot, const hpt_c
   std::unique_ptr<Request> r(new Request());
   r->id = server->next_id++;
   r->js.scene = &server->scenes[scene_slot]->h.scene;
+  r->scene_slot = scene_slot;
   r->js.camera = *camera;
   r->js.params = *params;
   r->want_accum = server->cfg.keep_accum != 0;
   r->rays = (int64_t)params->sample_x * params->supersample_x * params->sample_y *
             params->supersample_y;
   r->footprint = job_footprint(*params, r->want_accum);
+  r->small = r->rays * params->sample <= (int64_t)server->cfg.capacity;
   if (r->footprint > server->cfg.memory_budget)
     return fail(HPT_ERR_OUT_OF_MEMORY, "request needs %lld bytes, budget is %lld",
                 (long long)r->footprint, (long long)server->cfg.memory_budget);
@@ -492,9 +559,11 @@ hpt_status hpt_server_poll(hpt_server* server, uint64_t request_id, hpt_request_
     const hpt_status e = r->state == kCancelled ? HPT_ERR_CANCELLED : r->error;
     server->give_pinned(r->rgba, r->rgba_bytes);
     server->give_pinned(r->accum, r->accum_bytes);
+    const bool shed = r->shed;
     server->reqs.erase(request_id);
     return fail(e, "request %llu %s", (unsigned long long)request_id,
-                e == HPT_ERR_CANCELLED ? "was cancelled" : "failed");
+                shed ? "was shed by the overload policy (deadline)"
+                     : e == HPT_ERR_CANCELLED ? "was cancelled" : "failed");
   }
   // Running: a progressive preview divides by the samples completed so far
   // (paths finish out of order, so this is the fraction of finished paths).
@@ -529,6 +598,13 @@ hpt_status hpt_server_drain_completed(hpt_server* server, uint64_t* ids, int32_t
   server->finished_ids.erase(server->finished_ids.begin(), server->finished_ids.begin() + n);
   *count = n;
   return HPT_OK;
+}
+
+int64_t hpt_server_shed(const hpt_server* server) {
+  if (!server) return 0;
+  hpt_server* s = const_cast<hpt_server*>(server);
+  std::lock_guard<std::mutex> lk(s->mu);
+  return s->shed;
 }
 
 int32_t hpt_server_pending(const hpt_server* server) {

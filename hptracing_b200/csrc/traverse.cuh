@@ -244,6 +244,46 @@ HPT_HD void trav_init(const DevScene& s, const Ray& r, TravState& st, TravCold& 
   }
 }
 
+// Side of a split for the entry point: right when beyond it; a point on
+// the plane follows the direction, and a ray lying in the plane takes the
+// side of the current in-plane walk (tie_goes_right).
+HPT_HD bool goes_right(float p, float split, float dd, TravCold& tc, uint32_t axis) {
+  return p > split || (p == split && (dd > 0.f || (dd == 0.f && tie_goes_right(tc, axis))));
+}
+
+HPT_HD float pick(uint32_t axis, float x, float y, float z) {
+  return axis == 0 ? x : (axis == 1 ? y : z);
+}
+
+// One descent unit on the two-level records (DevWide): from `node`, one
+// 32-byte load decides up to two levels. Returns the leaf record index when
+// `node` is a leaf (node unchanged), else -1 with `node` moved down by
+// `levels` (1 when the first level reaches a leaf child, else 2). The
+// entry point is p = o + t_entry * d (kernel.cl:291 style, no FMA), the
+// same for every level, so the decisions are those of the binary walk.
+HPT_HD int wide_descend(const DevScene& s, int& node, const Ray& r, float t_entry, TravCold& tc,
+                        int& levels) {
+  const uint4* w = reinterpret_cast<const uint4*>(s.wide + node);
+  const uint4 a = ldg(w), b = ldg(w + 1);
+  levels = 0;
+  if (a.w & kWideLeaf) return (int)b.x;
+  uint32_t axis = a.w & 3u;
+  float p = rn_add(pick(axis, r.o.x, r.o.y, r.o.z), rn_mul(t_entry, pick(axis, r.d.x, r.d.y, r.d.z)));
+  const bool r0 = goes_right(p, as_float_u(a.x), pick(axis, r.d.x, r.d.y, r.d.z), tc, axis);
+  levels = 1;
+  if (a.w & (r0 ? kWideRightLeaf : kWideLeftLeaf)) {
+    node = (int)(r0 ? b.z : b.x);
+    return -1;
+  }
+  axis = (a.w >> (r0 ? 4 : 2)) & 3u;
+  p = rn_add(pick(axis, r.o.x, r.o.y, r.o.z), rn_mul(t_entry, pick(axis, r.d.x, r.d.y, r.d.z)));
+  const bool r1 =
+      goes_right(p, as_float_u(r0 ? a.z : a.y), pick(axis, r.d.x, r.d.y, r.d.z), tc, axis);
+  levels = 2;
+  node = (int)(r0 ? (r1 ? b.w : b.z) : (r1 ? b.y : b.x));
+  return -1;
+}
+
 // Node fetch with an optional shared-memory copy of the first n_smem nodes.
 HPT_HD uint2 fetch_node(const DevScene& s, const uint2* smem, int n_smem,
                                             int i) {
@@ -269,28 +309,45 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint
   const float py = rn_add(r.o.y, rn_mul(st.t_entry, r.d.y));
   const float pz = rn_add(r.o.z, rn_mul(st.t_entry, r.d.z));
   int node = st.node;
-  uint2 nd = fetch_node(s, smem, n_smem, node);
-  while ((nd.x >> 30) != kLeafKind) {
-    const uint32_t axis = nd.x >> 30;
-    const float split = as_float_u(nd.y);
-    const float p = axis == 0 ? px : (axis == 1 ? py : pz);
-    const float dd = axis == 0 ? r.d.x : (axis == 1 ? r.d.y : r.d.z);
-    const bool right =
-        p > split || (p == split && (dd > 0.f || (dd == 0.f && tie_goes_right(tc, axis))));
-    HPT_DCHECK(err, (int)(nd.x & kIndexMask) + 1 < s.num_nodes, 106, nd.x & kIndexMask,
-               { st.node = -1; return true; });
-    node = (int)(nd.x & kIndexMask) + (right ? 1 : 0);
-    nd = fetch_node(s, smem, n_smem, node);
-    ++cnt.nodes;
-    if (++st.steps > s.max_steps) {
-      hpt_atomic_or(&err->flags, 1u);
-      st.node = -1;
-      return true;
+  int leaf_idx;
+  if (n_smem == 0) {
+    // Two levels per load on the descent records.
+    while (true) {
+      int levels;
+      leaf_idx = wide_descend(s, node, r, st.t_entry, tc, levels);
+      if (leaf_idx >= 0) break;
+      HPT_DCHECK(err, node >= 0 && node < s.num_nodes, 106, node, { st.node = -1; return true; });
+      cnt.nodes += levels;
+      st.steps += levels;
+      if (st.steps > s.max_steps) {
+        hpt_atomic_or(&err->flags, 1u);
+        st.node = -1;
+        return true;
+      }
     }
+  } else {
+    uint2 nd = fetch_node(s, smem, n_smem, node);
+    while ((nd.x >> 30) != kLeafKind) {
+      const uint32_t axis = nd.x >> 30;
+      const float split = as_float_u(nd.y);
+      const float p = axis == 0 ? px : (axis == 1 ? py : pz);
+      const float dd = axis == 0 ? r.d.x : (axis == 1 ? r.d.y : r.d.z);
+      const bool right = goes_right(p, split, dd, tc, axis);
+      HPT_DCHECK(err, (int)(nd.x & kIndexMask) + 1 < s.num_nodes, 106, nd.x & kIndexMask,
+                 { st.node = -1; return true; });
+      node = (int)(nd.x & kIndexMask) + (right ? 1 : 0);
+      nd = fetch_node(s, smem, n_smem, node);
+      ++cnt.nodes;
+      if (++st.steps > s.max_steps) {
+        hpt_atomic_or(&err->flags, 1u);
+        st.node = -1;
+        return true;
+      }
+    }
+    leaf_idx = (int)(nd.x & kIndexMask);
   }
-  HPT_DCHECK(err, (int)(nd.x & kIndexMask) < s.num_leaves, 102, nd.x & kIndexMask,
-             { st.node = -1; return true; });
-  const DevLeaf* L = s.leaves + (nd.x & kIndexMask);
+  HPT_DCHECK(err, leaf_idx < s.num_leaves, 102, leaf_idx, { st.node = -1; return true; });
+  const DevLeaf* L = s.leaves + leaf_idx;
   const float4 L0 = ldg(reinterpret_cast<const float4*>(L));
   const float4 L1 = ldg(reinterpret_cast<const float4*>(L) + 1);
   // Exit distance and face (reciprocal multiplies; only the reference's box
@@ -417,32 +474,50 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, TravCold& tc, const uint
   const Ray& r = st.ray;
   if (st.phase == kStepDescend) {
     HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
-    const uint2 nd = fetch_node(s, smem, kSmem ? n_smem : 0, st.node);
-    if ((nd.x >> 30) != kLeafKind) {
-      // One descent step; the entry point p = o + t_entry * d on the split
-      // axis (kernel.cl:291 style, no FMA), as trav_leaf computes it.
-      const uint32_t axis = nd.x >> 30;
-      const float split = as_float_u(nd.y);
-      const float o = axis == 0 ? r.o.x : (axis == 1 ? r.o.y : r.o.z);
-      const float dd = axis == 0 ? r.d.x : (axis == 1 ? r.d.y : r.d.z);
-      const float p = rn_add(o, rn_mul(st.t_entry, dd));
-      const bool right =
-        p > split || (p == split && (dd > 0.f || (dd == 0.f && tie_goes_right(tc, axis))));
-      HPT_DCHECK(err, (int)(nd.x & kIndexMask) + 1 < s.num_nodes, 106, nd.x & kIndexMask,
-                 { st.node = -1; return true; });
-      st.node = (int)(nd.x & kIndexMask) + (right ? 1 : 0);
-      ++cnt.nodes;
-      if (++st.steps > s.max_steps) {
-        hpt_atomic_or(&err->flags, 1u);
-        st.node = -1;
-        return true;
+    int leaf;
+    if (!kSmem) {
+      // One descent unit: up to two levels from one 32-byte record.
+      int node = st.node, levels;
+      leaf = wide_descend(s, node, r, st.t_entry, tc, levels);
+      if (leaf < 0) {
+        HPT_DCHECK(err, node >= 0 && node < s.num_nodes, 106, node,
+                   { st.node = -1; return true; });
+        st.node = node;
+        cnt.nodes += levels;
+        st.steps += levels;
+        if (st.steps > s.max_steps) {
+          hpt_atomic_or(&err->flags, 1u);
+          st.node = -1;
+          return true;
+        }
+        return false;
       }
-      return false;
+    } else {
+      const uint2 nd = fetch_node(s, smem, n_smem, st.node);
+      if ((nd.x >> 30) != kLeafKind) {
+        // One descent step; the entry point p = o + t_entry * d on the split
+        // axis (kernel.cl:291 style, no FMA), as trav_leaf computes it.
+        const uint32_t axis = nd.x >> 30;
+        const float split = as_float_u(nd.y);
+        const float o = axis == 0 ? r.o.x : (axis == 1 ? r.o.y : r.o.z);
+        const float dd = axis == 0 ? r.d.x : (axis == 1 ? r.d.y : r.d.z);
+        const float p = rn_add(o, rn_mul(st.t_entry, dd));
+        const bool right = goes_right(p, split, dd, tc, axis);
+        HPT_DCHECK(err, (int)(nd.x & kIndexMask) + 1 < s.num_nodes, 106, nd.x & kIndexMask,
+                   { st.node = -1; return true; });
+        st.node = (int)(nd.x & kIndexMask) + (right ? 1 : 0);
+        ++cnt.nodes;
+        if (++st.steps > s.max_steps) {
+          hpt_atomic_or(&err->flags, 1u);
+          st.node = -1;
+          return true;
+        }
+        return false;
+      }
+      leaf = (int)(nd.x & kIndexMask);
     }
     // Leaf set-up: exit distance and face, triangle range.
-    HPT_DCHECK(err, (int)(nd.x & kIndexMask) < s.num_leaves, 102, nd.x & kIndexMask,
-               { st.node = -1; return true; });
-    const int leaf = (int)(nd.x & kIndexMask);
+    HPT_DCHECK(err, leaf < s.num_leaves, 102, leaf, { st.node = -1; return true; });
     const float4* L = reinterpret_cast<const float4*>(s.leaves + leaf);
     // The six ropes are read with the box (independent loads) so that the
     // exit needs no dependent load of its own.

@@ -416,7 +416,14 @@ typedef struct hpt_server_config {
   /* Keep each request's float accumulator for hpt_server_poll's accum_out
    * (costs 12 bytes per ray of device memory and copy-back). */
   int32_t keep_accum;
-  int32_t reserved[1];
+  /* Overload policy (0 = off). Requests with at most `capacity` paths
+   * (rays x spp) are latency-bound: they are served first-come first-served
+   * ahead of larger ones, admitted only while the latency-bound work
+   * already admitted is expected to finish within deadline_ms (per-scene
+   * service times learned from finished requests), and shed when still
+   * queued deadline_ms after submission (poll returns HPT_ERR_CANCELLED;
+   * hpt_server_shed counts them). */
+  int32_t deadline_ms;
 } hpt_server_config;
 
 typedef struct hpt_request_info {
@@ -454,6 +461,8 @@ hpt_status hpt_server_drain_completed(hpt_server* server, uint64_t* ids,
                                       int32_t max_ids, int32_t* count);
 /* Requests queued + running. */
 int32_t hpt_server_pending(const hpt_server* server);
+/* Requests shed by the overload policy (deadline_ms) since creation. */
+int64_t hpt_server_shed(const hpt_server* server);
 /* Cumulative device counters of the server's wavefront (intersect queries
  * including primary rays, shade calls, iterations, traversal work); `paths`
  * holds the number of completed requests. */

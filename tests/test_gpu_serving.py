@@ -202,3 +202,48 @@ def test_autotune_picks_a_valid_tuning_and_caches_it(scenes):
         finally:
             spheres.set_tuning(t0)
     assert np.array_equal(got, want)
+
+
+def test_overload_policy_sheds_late_requests_and_keeps_results(scenes):
+    """deadline_ms: latency-bound requests (<= capacity paths) are served
+    first-come first-served, admitted while the admitted ones are expected
+    to finish in time and shed when still queued past the deadline. A burst
+    of 64 requests with a 1 ms deadline: the first ones run (no service
+    estimate yet), later ones are shed (HPT_ERR_CANCELLED, counted by
+    hpt_server_shed), and every request that does complete is bit-identical
+    to the same request rendered alone. Without the policy nothing is shed."""
+    req = (1, S.ROOM_CAM, 96, 64, 1, 4, 6, (0, 0, 0), 300)
+    _, ref = _alone(scenes, req)
+    for deadline, expect_shed in ((1, True), (0, False)):
+        server = H.Server(max_jobs=8, memory_budget=1 << 30, capacity=1 << 16,
+                          deadline_ms=deadline)
+        slots = [server.add_scene(s) for s in scenes]
+        p = _params(req)
+        ids = [server.submit(slots[1], S.hp_camera(S.ROOM_CAM), p) for _ in range(64)]
+        done, shed = 0, 0
+        pending = set(ids)
+        for _ in range(200000):
+            if not pending:
+                break
+            server.pump(2)
+            for rid in list(pending):
+                acc = np.zeros((p.sample_x * p.sample_y, 3), np.float32)
+                try:
+                    st, _ = server.poll(rid, None, acc)
+                except H.HptError as e:
+                    assert e.status == 8 and "shed" in str(e), str(e)
+                    shed += 1
+                    pending.discard(rid)
+                    continue
+                if st == 0:
+                    assert np.array_equal(acc, ref)
+                    done += 1
+                    pending.discard(rid)
+        assert not pending
+        assert server.shed() == shed
+        print("deadline %d ms: %d done, %d shed" % (deadline, done, shed))
+        if expect_shed:
+            assert shed > 0 and done > 0
+        else:
+            assert shed == 0 and done == 64
+        server.close()
