@@ -27,9 +27,12 @@ constexpr uint32_t kIndexMask = 0x3FFFFFFFu;
 //  meta         bits 0-1 axis of the node, 2-3 of the left child, 4-5 of the
 //               right child; bit 6 / 7: left / right child is a leaf;
 //               bit 8: the node itself is a leaf
-//  next[0..3]   grandchildren LL, LR, RL, RR (DevNode indices); a leaf
-//               child's pair names the child itself; for a leaf node
-//               next[0] is its leaf record
+//  next[0..3]   grandchildren LL, LR, RL, RR: a DevNode index, or
+//               kLeafRef | leaf record for a leaf (a leaf child's pair names
+//               the child's leaf twice); for a leaf node next[0] is its leaf
+//               record
+// Node references in descent records, ropes and start hints name a leaf by
+// its record (kLeafRef | index), so reaching a leaf needs no node load.
 struct DevWide {
   float split[3];
   uint32_t meta;
@@ -39,6 +42,7 @@ static_assert(sizeof(DevWide) == 32, "32-byte descent record");
 constexpr uint32_t kWideLeftLeaf = 1u << 6;
 constexpr uint32_t kWideRightLeaf = 1u << 7;
 constexpr uint32_t kWideLeaf = 1u << 8;
+constexpr int32_t kLeafRef = 1 << 30;
 
 // Leaf record, 64 bytes (4 x 16 B):
 //  [0] lo.x lo.y lo.z  first entry in leaf_refs (int bits)

@@ -113,11 +113,11 @@ struct TravCold {
   f3 inv_d;           // 1 / d (exit distances only; the filter divides)
   float t_end;        // scene exit distance
   float slack;        // world-space rounding slack in t units
-  int32_t best_node;  // leaf node where the best hit was found
+  int32_t best_node;  // leaf of the best hit (kLeafRef | leaf record)
   // trav_step's current leaf:
   int32_t leaf;       // leaf record
-  int32_t leaf_node;  // its node index (reported as best_node)
-  int32_t rope;       // node behind the exit face, -1 when there is none
+  int32_t leaf_node;  // kLeafRef | leaf (reported as best_node)
+  int32_t rope;       // node reference behind the exit face, -1 when none
   int32_t pierced;    // reference box test of the leaf: -1 not evaluated yet
   float t_exit;
   // Rays that lie exactly in a split plane (see trav_finish):
@@ -172,7 +172,8 @@ struct TravCount {
   uint32_t nodes, leaves, tris, repeats;
 };
 
-// Starts a query. start_node (>= 0) names a leaf node the origin is
+// Starts a query. start_node (>= 0) names a leaf (a leaf reference, or the
+// DevNode index of a leaf) the origin is
 // expected to lie in (the leaf of the previous hit): if its box contains the
 // origin the walk starts there instead of descending from the root.
 HPT_HD void trav_init(const DevScene& s, const Ray& r, TravState& st, TravCold& tc,
@@ -223,25 +224,36 @@ HPT_HD void trav_init(const DevScene& s, const Ray& r, TravState& st, TravCold& 
   tc.t_start = t0;
   tc.ties = (d[0] == 0.f ? 1 : 0) | (d[1] == 0.f ? 2 : 0) | (d[2] == 0.f ? 4 : 0);
   st.node = 0;
-  if (start_node > 0 && start_node < s.num_nodes) {
+  // The hinted leaf: a leaf reference, or the DevNode index of a leaf.
+  int hint = -1;
+  if (start_node >= 0 && (start_node & kLeafRef)) {
+    if ((start_node & ~kLeafRef) < s.num_leaves) hint = start_node & ~kLeafRef;
+  } else if (start_node > 0 && start_node < s.num_nodes) {
     const uint2 nd = ldg(reinterpret_cast<const uint2*>(s.nodes) + start_node);
-    if ((nd.x >> 30) == kLeafKind) {
-      const float4* L = reinterpret_cast<const float4*>(s.leaves + (nd.x & kIndexMask));
-      const float4 lo = ldg(L), hi = ldg(L + 1);
-      // A hinted start skips the descents from the root, and with them any
-      // split plane the ray lies in; such a plane bounds the leaf, so along a
-      // zero direction component the origin must lie strictly inside.
-      const int z = tc.ties;
-      const bool off_planes = (!(z & 1) || (o[0] > lo.x && o[0] < hi.x)) &&
-                              (!(z & 2) || (o[1] > lo.y && o[1] < hi.y)) &&
-                              (!(z & 4) || (o[2] > lo.z && o[2] < hi.z));
-      if (o[0] >= lo.x && o[0] <= hi.x && o[1] >= lo.y && o[1] <= hi.y && o[2] >= lo.z &&
-          o[2] <= hi.z && off_planes) {
-        st.node = start_node;
-        st.t_entry = 0.f;
-      }
+    if ((nd.x >> 30) == kLeafKind) hint = (int)(nd.x & kIndexMask);
+  }
+  if (hint >= 0) {
+    const float4* L = reinterpret_cast<const float4*>(s.leaves + hint);
+    const float4 lo = ldg(L), hi = ldg(L + 1);
+    // A hinted start skips the descents from the root, and with them any
+    // split plane the ray lies in; such a plane bounds the leaf, so along a
+    // zero direction component the origin must lie strictly inside.
+    const int z = tc.ties;
+    const bool off_planes = (!(z & 1) || (o[0] > lo.x && o[0] < hi.x)) &&
+                            (!(z & 2) || (o[1] > lo.y && o[1] < hi.y)) &&
+                            (!(z & 4) || (o[2] > lo.z && o[2] < hi.z));
+    if (o[0] >= lo.x && o[0] <= hi.x && o[1] >= lo.y && o[1] <= hi.y && o[2] >= lo.z &&
+        o[2] <= hi.z && off_planes) {
+      st.node = kLeafRef | hint;
+      st.t_entry = 0.f;
     }
   }
+}
+
+// A node reference (DevNode index, or kLeafRef | leaf record) inside the
+// scene's arrays.
+HPT_HD bool valid_ref(const DevScene& s, int ref) {
+  return ref >= 0 && ((ref & kLeafRef) ? (ref & ~kLeafRef) < s.num_leaves : ref < s.num_nodes);
 }
 
 // Side of a split for the entry point: right when beyond it; a point on
@@ -263,9 +275,10 @@ HPT_HD float pick(uint32_t axis, float x, float y, float z) {
 // same for every level, so the decisions are those of the binary walk.
 HPT_HD int wide_descend(const DevScene& s, int& node, const Ray& r, float t_entry, TravCold& tc,
                         int& levels) {
+  levels = 0;
+  if (node & kLeafRef) return node & ~kLeafRef;  // a leaf reference: no load
   const uint4* w = reinterpret_cast<const uint4*>(s.wide + node);
   const uint4 a = ldg(w), b = ldg(w + 1);
-  levels = 0;
   if (a.w & kWideLeaf) return (int)b.x;
   uint32_t axis = a.w & 3u;
   float p = rn_add(pick(axis, r.o.x, r.o.y, r.o.z), rn_mul(t_entry, pick(axis, r.d.x, r.d.y, r.d.z)));
@@ -302,7 +315,7 @@ template <bool kUV = false>
 HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint2* smem,
                       int n_smem, DevErr* err, TravCount& cnt) {
   if (st.node < 0) return true;
-  HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
+  HPT_DCHECK(err, valid_ref(s, st.node), 101, st.node, { st.node = -1; return true; });
   const Ray& r = st.ray;
   // Entry point p = o + t_entry * d (kernel.cl:291 style, no FMA).
   const float px = rn_add(r.o.x, rn_mul(st.t_entry, r.d.x));
@@ -316,7 +329,7 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint
       int levels;
       leaf_idx = wide_descend(s, node, r, st.t_entry, tc, levels);
       if (leaf_idx >= 0) break;
-      HPT_DCHECK(err, node >= 0 && node < s.num_nodes, 106, node, { st.node = -1; return true; });
+      HPT_DCHECK(err, valid_ref(s, node), 106, node, { st.node = -1; return true; });
       cnt.nodes += levels;
       st.steps += levels;
       if (st.steps > s.max_steps) {
@@ -325,6 +338,8 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint
         return true;
       }
     }
+  } else if (node & kLeafRef) {
+    leaf_idx = node & ~kLeafRef;
   } else {
     uint2 nd = fetch_node(s, smem, n_smem, node);
     while ((nd.x >> 30) != kLeafKind) {
@@ -426,7 +441,7 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint
             st.best.u = u;
             st.best.v = v;
           }
-          tc.best_node = node;
+          tc.best_node = kLeafRef | leaf_idx;
         }
       }
     }
@@ -443,7 +458,7 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint
     st.node = -1;
     return true;
   }
-  HPT_DCHECK(err, rope < s.num_nodes, 105, rope, { st.node = -1; return true; });
+  HPT_DCHECK(err, valid_ref(s, rope), 105, rope, { st.node = -1; return true; });
   st.node = rope;
   st.t_entry = fmaxf(st.t_entry, t_exit);
   return false;
@@ -473,15 +488,14 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, TravCold& tc, const uint
   if (st.node < 0) return true;
   const Ray& r = st.ray;
   if (st.phase == kStepDescend) {
-    HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
+    HPT_DCHECK(err, valid_ref(s, st.node), 101, st.node, { st.node = -1; return true; });
     int leaf;
     if (!kSmem) {
       // One descent unit: up to two levels from one 32-byte record.
       int node = st.node, levels;
       leaf = wide_descend(s, node, r, st.t_entry, tc, levels);
       if (leaf < 0) {
-        HPT_DCHECK(err, node >= 0 && node < s.num_nodes, 106, node,
-                   { st.node = -1; return true; });
+        HPT_DCHECK(err, valid_ref(s, node), 106, node, { st.node = -1; return true; });
         st.node = node;
         cnt.nodes += levels;
         st.steps += levels;
@@ -492,6 +506,8 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, TravCold& tc, const uint
         }
         return false;
       }
+    } else if (st.node & kLeafRef) {
+      leaf = st.node & ~kLeafRef;
     } else {
       const uint2 nd = fetch_node(s, smem, n_smem, st.node);
       if ((nd.x >> 30) != kLeafKind) {
@@ -553,7 +569,7 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, TravCold& tc, const uint
     st.k = begin;
     st.end = begin + count;
     tc.leaf = leaf;
-    tc.leaf_node = st.node;
+    tc.leaf_node = kLeafRef | leaf;
     tc.rope = face == 0 ? R03.x : face == 1 ? R03.y : face == 2 ? R03.z
             : face == 3 ? R03.w : face == 4 ? R45.x : face == 5 ? R45.y : -1;
     tc.t_exit = t_exit;
@@ -630,7 +646,7 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, TravCold& tc, const uint
     st.node = -1;
     return true;
   }
-  HPT_DCHECK(err, rope < s.num_nodes, 105, rope, { st.node = -1; return true; });
+  HPT_DCHECK(err, valid_ref(s, rope), 105, rope, { st.node = -1; return true; });
   st.node = rope;
   st.t_entry = fmaxf(st.t_entry, tc.t_exit);
   return false;
