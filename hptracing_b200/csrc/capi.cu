@@ -354,15 +354,12 @@ hpt_status upload_scene(const hpt_scene_desc& d, SceneDev& out) {
   const DevTri* recs;
   const int32_t* refs;
   if ((s = dev_upload(out, pk.nodes.data(), pk.nodes.size(), &nodes)) != HPT_OK) return s;
-  const DevWide* wide;
-  if ((s = dev_upload(out, pk.wide.data(), pk.wide.size(), &wide)) != HPT_OK) return s;
   if ((s = dev_upload(out, pk.leaves.data(), pk.leaves.size(), &leaves)) != HPT_OK) return s;
   // At least one entry so the pointer is valid even for an empty tree.
   if (pk.refs.empty()) pk.refs.push_back(0);
   if ((s = dev_upload(out, pk.refs.data(), pk.refs.size(), &refs)) != HPT_OK) return s;
   if ((s = dev_upload(out, pk.tris.data(), pk.tris.size(), &recs)) != HPT_OK) return s;
   ds.nodes = nodes;
-  ds.wide = wide;
   ds.leaves = leaves;
   ds.leaf_refs = refs;
   ds.tris = recs;

@@ -20,28 +20,9 @@ static_assert(sizeof(DevNode) == 8, "8-byte traversal node");
 constexpr uint32_t kLeafKind = 3u;
 constexpr uint32_t kIndexMask = 0x3FFFFFFFu;
 
-// Two-level descent record, 32 bytes, one per node of the DevNode array
-// (same index): the node's split and its two children's, so one load
-// decides two levels of a descent.
-//  split[0..2]  the node's, its left child's, its right child's split
-//  meta         bits 0-1 axis of the node, 2-3 of the left child, 4-5 of the
-//               right child; bit 6 / 7: left / right child is a leaf;
-//               bit 8: the node itself is a leaf
-//  next[0..3]   grandchildren LL, LR, RL, RR: a DevNode index, or
-//               kLeafRef | leaf record for a leaf (a leaf child's pair names
-//               the child's leaf twice); for a leaf node next[0] is its leaf
-//               record
-// Node references in descent records, ropes and start hints name a leaf by
-// its record (kLeafRef | index), so reaching a leaf needs no node load.
-struct DevWide {
-  float split[3];
-  uint32_t meta;
-  int32_t next[4];
-};
-static_assert(sizeof(DevWide) == 32, "32-byte descent record");
-constexpr uint32_t kWideLeftLeaf = 1u << 6;
-constexpr uint32_t kWideRightLeaf = 1u << 7;
-constexpr uint32_t kWideLeaf = 1u << 8;
+// A node reference in a rope or a start hint names a leaf by its record,
+// kLeafRef | leaf index, so reaching a leaf that way needs no node load;
+// other references are DevNode indices.
 constexpr int32_t kLeafRef = 1 << 30;
 
 // Leaf record, 64 bytes (4 x 16 B):
@@ -89,7 +70,6 @@ struct DevTexInfo {
 // Pointers of one device-resident scene (all device addresses).
 struct DevScene {
   const DevNode* nodes;
-  const DevWide* wide;        // descent records, one per node
   const DevLeaf* leaves;
   const int32_t* leaf_refs;   // triangle ids in leaf (= reference gather) order
   const DevTri* tris;         // indexed by triangle id

@@ -782,6 +782,9 @@ hpt_tuning default_tuning() {
   t.smem_nodes = 0;
   t.use_graph = 0;
   t.trav_steps = 24;
+  // Shading at 4 blocks of 256 per SM (64 registers): 7.0 instead of 8.4 ms
+  // per spheres frame at the natural 106-register allocation (2 blocks).
+  t.shade_min_blocks = 4;
   return t;
 }
 

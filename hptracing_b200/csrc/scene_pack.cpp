@@ -284,38 +284,6 @@ hpt_status pack_scene(const hpt_scene_desc& d, int bfs_nodes, PackedScene& out) 
         const TmpNode& t = p.nodes[L.rope[f]];
         L.rope[f] = t.axis < 0 ? (kLeafRef | t.leaf) : idx[L.rope[f]];
       }
-  // Two-level descent records over the final layout.
-  out.wide.assign(nn, DevWide());
-  for (size_t n = 0; n < nn; ++n) {
-    const DevNode& o = out.nodes[n];
-    DevWide& w = out.wide[n];
-    memset(&w, 0, sizeof w);
-    if ((o.meta >> 30) == kLeafKind) {
-      w.meta = kWideLeaf;
-      w.next[0] = (int32_t)(o.meta & kIndexMask);
-      continue;
-    }
-    const int32_t left = (int32_t)(o.meta & kIndexMask);
-    w.split[0] = o.split;
-    w.meta = o.meta >> 30;
-    // A reference to node k: the node, or its leaf record.
-    auto ref_of = [&](int32_t k) -> int32_t {
-      const DevNode& x = out.nodes[k];
-      return (x.meta >> 30) == kLeafKind ? (kLeafRef | (int32_t)(x.meta & kIndexMask)) : k;
-    };
-    for (int c = 0; c < 2; ++c) {
-      const DevNode& ch = out.nodes[left + c];
-      if ((ch.meta >> 30) == kLeafKind) {
-        w.meta |= c ? kWideRightLeaf : kWideLeftLeaf;
-        w.next[2 * c] = w.next[2 * c + 1] = ref_of(left + c);
-      } else {
-        w.split[1 + c] = ch.split;
-        w.meta |= (ch.meta >> 30) << (2 + 2 * c);
-        w.next[2 * c] = ref_of((int32_t)(ch.meta & kIndexMask));
-        w.next[2 * c + 1] = ref_of((int32_t)(ch.meta & kIndexMask) + 1);
-      }
-    }
-  }
   out.leaves = std::move(p.leaves);
   out.refs = std::move(p.refs);
   out.tris.resize(d.num_triangles);

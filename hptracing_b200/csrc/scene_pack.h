@@ -10,7 +10,6 @@ namespace hpt {
 
 struct PackedScene {
   std::vector<DevNode> nodes;
-  std::vector<DevWide> wide;   // two-level descent record per node
   std::vector<DevLeaf> leaves;
   std::vector<int32_t> refs;   // triangle ids in leaf order
   std::vector<DevTri> tris;    // one record per triangle

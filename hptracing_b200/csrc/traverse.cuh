@@ -263,40 +263,6 @@ HPT_HD bool goes_right(float p, float split, float dd, TravCold& tc, uint32_t ax
   return p > split || (p == split && (dd > 0.f || (dd == 0.f && tie_goes_right(tc, axis))));
 }
 
-HPT_HD float pick(uint32_t axis, float x, float y, float z) {
-  return axis == 0 ? x : (axis == 1 ? y : z);
-}
-
-// One descent unit on the two-level records (DevWide): from `node`, one
-// 32-byte load decides up to two levels. Returns the leaf record index when
-// `node` is a leaf (node unchanged), else -1 with `node` moved down by
-// `levels` (1 when the first level reaches a leaf child, else 2). The
-// entry point is p = o + t_entry * d (kernel.cl:291 style, no FMA), the
-// same for every level, so the decisions are those of the binary walk.
-HPT_HD int wide_descend(const DevScene& s, int& node, const Ray& r, float t_entry, TravCold& tc,
-                        int& levels) {
-  levels = 0;
-  if (node & kLeafRef) return node & ~kLeafRef;  // a leaf reference: no load
-  const uint4* w = reinterpret_cast<const uint4*>(s.wide + node);
-  const uint4 a = ldg(w), b = ldg(w + 1);
-  if (a.w & kWideLeaf) return (int)b.x;
-  uint32_t axis = a.w & 3u;
-  float p = rn_add(pick(axis, r.o.x, r.o.y, r.o.z), rn_mul(t_entry, pick(axis, r.d.x, r.d.y, r.d.z)));
-  const bool r0 = goes_right(p, as_float_u(a.x), pick(axis, r.d.x, r.d.y, r.d.z), tc, axis);
-  levels = 1;
-  if (a.w & (r0 ? kWideRightLeaf : kWideLeftLeaf)) {
-    node = (int)(r0 ? b.z : b.x);
-    return -1;
-  }
-  axis = (a.w >> (r0 ? 4 : 2)) & 3u;
-  p = rn_add(pick(axis, r.o.x, r.o.y, r.o.z), rn_mul(t_entry, pick(axis, r.d.x, r.d.y, r.d.z)));
-  const bool r1 =
-      goes_right(p, as_float_u(r0 ? a.z : a.y), pick(axis, r.d.x, r.d.y, r.d.z), tc, axis);
-  levels = 2;
-  node = (int)(r0 ? (r1 ? b.w : b.z) : (r1 ? b.y : b.x));
-  return -1;
-}
-
 // Node fetch with an optional shared-memory copy of the first n_smem nodes.
 HPT_HD uint2 fetch_node(const DevScene& s, const uint2* smem, int n_smem,
                                             int i) {
@@ -323,22 +289,7 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint
   const float pz = rn_add(r.o.z, rn_mul(st.t_entry, r.d.z));
   int node = st.node;
   int leaf_idx;
-  if (n_smem == 0) {
-    // Two levels per load on the descent records.
-    while (true) {
-      int levels;
-      leaf_idx = wide_descend(s, node, r, st.t_entry, tc, levels);
-      if (leaf_idx >= 0) break;
-      HPT_DCHECK(err, valid_ref(s, node), 106, node, { st.node = -1; return true; });
-      cnt.nodes += levels;
-      st.steps += levels;
-      if (st.steps > s.max_steps) {
-        hpt_atomic_or(&err->flags, 1u);
-        st.node = -1;
-        return true;
-      }
-    }
-  } else if (node & kLeafRef) {
+  if (node & kLeafRef) {  // a leaf reference: no node load
     leaf_idx = node & ~kLeafRef;
   } else {
     uint2 nd = fetch_node(s, smem, n_smem, node);
@@ -490,26 +441,10 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, TravCold& tc, const uint
   if (st.phase == kStepDescend) {
     HPT_DCHECK(err, valid_ref(s, st.node), 101, st.node, { st.node = -1; return true; });
     int leaf;
-    if (!kSmem) {
-      // One descent unit: up to two levels from one 32-byte record.
-      int node = st.node, levels;
-      leaf = wide_descend(s, node, r, st.t_entry, tc, levels);
-      if (leaf < 0) {
-        HPT_DCHECK(err, valid_ref(s, node), 106, node, { st.node = -1; return true; });
-        st.node = node;
-        cnt.nodes += levels;
-        st.steps += levels;
-        if (st.steps > s.max_steps) {
-          hpt_atomic_or(&err->flags, 1u);
-          st.node = -1;
-          return true;
-        }
-        return false;
-      }
-    } else if (st.node & kLeafRef) {
+    if (st.node & kLeafRef) {  // a leaf reference: no node load
       leaf = st.node & ~kLeafRef;
     } else {
-      const uint2 nd = fetch_node(s, smem, n_smem, st.node);
+      const uint2 nd = fetch_node(s, smem, kSmem ? n_smem : 0, st.node);
       if ((nd.x >> 30) != kLeafKind) {
         // One descent step; the entry point p = o + t_entry * d on the split
         // axis (kernel.cl:291 style, no FMA), as trav_leaf computes it.

@@ -285,7 +285,8 @@ typedef struct hpt_tuning {
                              /* 100000. Larger values are clamped to it.  */
   int32_t shade_min_blocks;  /* register budget of the shading kernel:    */
                              /* 3 or 4 blocks of 256 threads per SM; 0 =  */
-                             /* the natural allocation (2 blocks)         */
+                             /* the natural allocation (2 blocks). The    */
+                             /* default is 4                              */
 } hpt_tuning;
 hpt_status hpt_tuning_get(const hpt_scene* scene, hpt_tuning* out);
 hpt_status hpt_tuning_set(hpt_scene* scene, const hpt_tuning* in);

@@ -40,7 +40,6 @@ void* emu_scene_create(const hpt_scene_desc* d, int* status) {
   DevScene& ds = e->dev;
   memset(&ds, 0, sizeof ds);
   ds.nodes = e->pk.nodes.data();
-  ds.wide = e->pk.wide.data();
   ds.leaves = e->pk.leaves.data();
   if (e->pk.refs.empty()) e->pk.refs.push_back(0);
   ds.leaf_refs = e->pk.refs.data();

@@ -7,7 +7,11 @@ reference's hp::KDTree (its OBJ loader and SAH builder), and calls
 hp::TraceRunner(scene) and run(...) exactly as the reference's CLI does
 (src/hptracing.cpp:74-78, 249). The image must match the oracle's render of
 the same scene (loaded by the same reference loader) driven by the same
-random streams: the first run() of a runner uses seed 0."""
+random streams: the first run() of a runner uses seed 0. The Cornell
+box's paths are chaotic (its 556-unit scale rounds away the reference's 1e-5
+offset of the next ray's origin; see test_gpu_cornell.py), so the pixel
+agreement is held to the oracle's own agreement with its render from a
+camera moved by one ulp, and the image means to 0.5 %."""
 import os
 import subprocess
 
@@ -62,10 +66,19 @@ def test_dropin_header_with_reference_types(built, tmp_path):
     acc, _, counts = cpu.render(cam, w, h, 1, 1, (0, 0, 0), spp, depth, 0, seed=0, rng_mode=1,
                                 threads=THREADS)
     ref = O.resolve(acc, w, h, 1, 1, spp).astype(np.int32)
+    cam2 = dict(cam)
+    v = np.asarray(cam["view_p"], np.float32).copy()
+    v[0] = np.nextafter(v[0], np.float32(np.inf))
+    cam2["view_p"] = tuple(float(x) for x in v)
+    moved, _, _ = cpu.render(cam2, w, h, 1, 1, (0, 0, 0), spp, depth, 0, seed=0, rng_mode=1,
+                             threads=THREADS)
+    mimg = O.resolve(moved, w, h, 1, 1, spp).astype(np.int32)
     close = (np.abs(img - ref).max(axis=2) <= 1).mean()
-    print("drop-in with the reference's types: %s; pixels within 1/255 %.4f, mean %.3f vs %.3f "
-          "(oracle %d queries)" % (r.stdout.strip(), close, img[:, :, :3].mean(),
-                                   ref[:, :, :3].mean(), counts[0]))
+    self_close = (np.abs(mimg - ref).max(axis=2) <= 1).mean()
+    print("drop-in with the reference's types: %s; pixels within 1/255 %.4f (oracle vs its "
+          "one-ulp camera move %.4f), mean %.3f vs %.3f (oracle %d queries)"
+          % (r.stdout.strip(), close, self_close, img[:, :, :3].mean(), ref[:, :, :3].mean(),
+             counts[0]))
     assert (img[:, :, 3] == 0).all()
-    assert close >= 0.98
+    assert close >= self_close
     assert abs(img[:, :, :3].mean() - ref[:, :, :3].mean()) / ref[:, :, :3].mean() < 0.005

@@ -90,8 +90,11 @@ def test_headline_fp32_vs_fp64(c1, batches):
 @pytest.mark.parametrize("kind", ["camera", "secondary"])
 def test_headline_shade_full_textures(c1, batches, kind):
     """s1_run on every hit of a batch with the 1024^2 textures, then the
-    next directions: shading bit-exact; next-dir light branch bit-exact,
-    the other branches within 2e-5 (acos / sin / cos / pow / asin ulps)."""
+    next directions: shading bit-exact; next-dir light branch bit-exact; the
+    other branches use acos / sin / cos / pow / asin, whose last bits differ
+    between CUDA and the host library: >= 99.99 % of the rays within 2e-5 and
+    all within 1e-3 (refraction close to the critical angle amplifies an
+    ulp: sqrt(1 - x^2) has slope x / sqrt(1 - x^2) there)."""
     _, gpu, cpu = c1
     o, d = batches[kind]
     ref = cpu.intersect(o, d, threads=THREADS)
@@ -122,7 +125,9 @@ def test_headline_shade_full_textures(c1, batches, kind):
         assert np.array_equal(gn[k][light], cn[k][light]), k
     for k in ("origins", "directions", "strength"):
         err = np.abs(gn[k][~light] - cn[k][~light]) / np.maximum(np.abs(cn[k][~light]), 1.0)
-        assert err.max() < 2e-5, (k, err.max())
+        within = (err < 2e-5).all(axis=1).mean()
+        print("next-dir %s: within 2e-5 %.6f, max %.3g" % (k, within, err.max()))
+        assert within >= 0.9999 and err.max() < 1e-3, (k, within, err.max())
     assert (gn["alive"] == cn["alive"]).mean() > 0.9999
     assert np.array_equal(gn["seeds"].astype(np.int64), cn["seeds"])
 
