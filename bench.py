@@ -513,6 +513,17 @@ def batch_c3(world, rank):
     t_max = max(m for m, _ in per_job)
     best_rate = max(q / m for m, q in per_job if m > 0)
     bound = sum(m for m, _ in per_job) / max(t_max, sum(q for _, q in per_job) / best_rate)
+    # A tighter bound: a query costs what it costs in its scene family, so
+    # the batch needs at least sum over jobs of queries / (that family's
+    # rate with the device full), the rate taken from the family's job with
+    # the most queries (the one that fills the wavefront best).
+    fam_rate = {}
+    for j, (m, q) in zip(jobs, per_job):
+        f = j["family"]
+        if m > 0 and (f not in fam_rate or q > fam_rate[f][1]):
+            fam_rate[f] = (q / m, q)
+    fam_bound = sum(m for m, _ in per_job) / max(
+        t_max, sum(q / fam_rate[j["family"]][0] for j, (_, q) in zip(jobs, per_job)))
     line = {
         "metric": "Mrays/s batched vs plain (C3, 32 mixed jobs)", "mode": "batch",
         "value": q_b / ms_b / 1e3, "unit": "Mrays/s", "plain": q_p / ms_p / 1e3,
@@ -523,6 +534,11 @@ def batch_c3(world, rank):
         "accumulators_bit_identical": same,
         "largest_job_share_of_work": max(work) / sum(work),
         "amdahl_bound": bound if world == 1 else None,
+        "family_rate_bound": fam_bound if world == 1 else None,
+        "family_rate_Mrays_per_s": {str(f): r[0] / 1e3 for f, r in fam_rate.items()},
+        "plain_per_job": [{"family": j["family"], "tris": j["tris"], "res": j["res"],
+                           "spp": j["spp"], "depth": j["depth"], "ms": m, "queries": q}
+                          for j, (m, q) in zip(jobs, per_job)],
         "largest_job_share_of_plain_ms": t_max / sum(m for m, _ in per_job),
         "tuning": {"capacity": tune.capacity, "isect_block": tune.isect_block,
                    "isect_min_blocks": tune.isect_min_blocks, "refill": tune.refill_chunk,
@@ -932,7 +948,8 @@ def main():
             line["batch"] = {k: b[k] for k in (
                 "metric", "value", "plain", "speedup", "unit", "ms_batched", "ms_plain",
                 "queries", "e2e", "accumulators_bit_identical", "largest_job_share_of_work",
-                "largest_job_share_of_plain_ms", "amdahl_bound", "tuning", "scene_build_s",
+                "largest_job_share_of_plain_ms", "amdahl_bound", "family_rate_bound",
+                "family_rate_Mrays_per_s", "tuning", "scene_build_s",
                 "jobs_per_rank") if k in b}
         if world == 1:
             import hptracing_b200 as H

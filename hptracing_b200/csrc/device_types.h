@@ -20,11 +20,6 @@ static_assert(sizeof(DevNode) == 8, "8-byte traversal node");
 constexpr uint32_t kLeafKind = 3u;
 constexpr uint32_t kIndexMask = 0x3FFFFFFFu;
 
-// A node reference in a rope or a start hint names a leaf by its record,
-// kLeafRef | leaf index, so reaching a leaf that way needs no node load;
-// other references are DevNode indices.
-constexpr int32_t kLeafRef = 1 << 30;
-
 // Leaf record, 64 bytes (4 x 16 B):
 //  [0] lo.x lo.y lo.z  first entry in leaf_refs (int bits)
 //  [1] hi.x hi.y hi.z  number of entries (int bits)

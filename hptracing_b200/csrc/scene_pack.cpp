@@ -277,13 +277,9 @@ hpt_status pack_scene(const hpt_scene_desc& d, int bfs_nodes, PackedScene& out) 
       o.split = t.split;
     }
   }
-  // A rope to a leaf names the leaf record itself.
   for (DevLeaf& L : p.leaves)
     for (int f = 0; f < 6; ++f)
-      if (L.rope[f] >= 0) {
-        const TmpNode& t = p.nodes[L.rope[f]];
-        L.rope[f] = t.axis < 0 ? (kLeafRef | t.leaf) : idx[L.rope[f]];
-      }
+      if (L.rope[f] >= 0) L.rope[f] = idx[L.rope[f]];
   out.leaves = std::move(p.leaves);
   out.refs = std::move(p.refs);
   out.tris.resize(d.num_triangles);

@@ -113,11 +113,11 @@ struct TravCold {
   f3 inv_d;           // 1 / d (exit distances only; the filter divides)
   float t_end;        // scene exit distance
   float slack;        // world-space rounding slack in t units
-  int32_t best_node;  // leaf of the best hit (kLeafRef | leaf record)
+  int32_t best_node;  // leaf node where the best hit was found
   // trav_step's current leaf:
   int32_t leaf;       // leaf record
-  int32_t leaf_node;  // kLeafRef | leaf (reported as best_node)
-  int32_t rope;       // node reference behind the exit face, -1 when none
+  int32_t leaf_node;  // its node index (reported as best_node)
+  int32_t rope;       // node behind the exit face, -1 when there is none
   int32_t pierced;    // reference box test of the leaf: -1 not evaluated yet
   float t_exit;
   // Rays that lie exactly in a split plane (see trav_finish):
@@ -172,8 +172,7 @@ struct TravCount {
   uint32_t nodes, leaves, tris, repeats;
 };
 
-// Starts a query. start_node (>= 0) names a leaf (a leaf reference, or the
-// DevNode index of a leaf) the origin is
+// Starts a query. start_node (>= 0) names a leaf node the origin is
 // expected to lie in (the leaf of the previous hit): if its box contains the
 // origin the walk starts there instead of descending from the root.
 HPT_HD void trav_init(const DevScene& s, const Ray& r, TravState& st, TravCold& tc,
@@ -224,43 +223,25 @@ HPT_HD void trav_init(const DevScene& s, const Ray& r, TravState& st, TravCold& 
   tc.t_start = t0;
   tc.ties = (d[0] == 0.f ? 1 : 0) | (d[1] == 0.f ? 2 : 0) | (d[2] == 0.f ? 4 : 0);
   st.node = 0;
-  // The hinted leaf: a leaf reference, or the DevNode index of a leaf.
-  int hint = -1;
-  if (start_node >= 0 && (start_node & kLeafRef)) {
-    if ((start_node & ~kLeafRef) < s.num_leaves) hint = start_node & ~kLeafRef;
-  } else if (start_node > 0 && start_node < s.num_nodes) {
+  if (start_node > 0 && start_node < s.num_nodes) {
     const uint2 nd = ldg(reinterpret_cast<const uint2*>(s.nodes) + start_node);
-    if ((nd.x >> 30) == kLeafKind) hint = (int)(nd.x & kIndexMask);
-  }
-  if (hint >= 0) {
-    const float4* L = reinterpret_cast<const float4*>(s.leaves + hint);
-    const float4 lo = ldg(L), hi = ldg(L + 1);
-    // A hinted start skips the descents from the root, and with them any
-    // split plane the ray lies in; such a plane bounds the leaf, so along a
-    // zero direction component the origin must lie strictly inside.
-    const int z = tc.ties;
-    const bool off_planes = (!(z & 1) || (o[0] > lo.x && o[0] < hi.x)) &&
-                            (!(z & 2) || (o[1] > lo.y && o[1] < hi.y)) &&
-                            (!(z & 4) || (o[2] > lo.z && o[2] < hi.z));
-    if (o[0] >= lo.x && o[0] <= hi.x && o[1] >= lo.y && o[1] <= hi.y && o[2] >= lo.z &&
-        o[2] <= hi.z && off_planes) {
-      st.node = kLeafRef | hint;
-      st.t_entry = 0.f;
+    if ((nd.x >> 30) == kLeafKind) {
+      const float4* L = reinterpret_cast<const float4*>(s.leaves + (nd.x & kIndexMask));
+      const float4 lo = ldg(L), hi = ldg(L + 1);
+      // A hinted start skips the descents from the root, and with them any
+      // split plane the ray lies in; such a plane bounds the leaf, so along a
+      // zero direction component the origin must lie strictly inside.
+      const int z = tc.ties;
+      const bool off_planes = (!(z & 1) || (o[0] > lo.x && o[0] < hi.x)) &&
+                              (!(z & 2) || (o[1] > lo.y && o[1] < hi.y)) &&
+                              (!(z & 4) || (o[2] > lo.z && o[2] < hi.z));
+      if (o[0] >= lo.x && o[0] <= hi.x && o[1] >= lo.y && o[1] <= hi.y && o[2] >= lo.z &&
+          o[2] <= hi.z && off_planes) {
+        st.node = start_node;
+        st.t_entry = 0.f;
+      }
     }
   }
-}
-
-// A node reference (DevNode index, or kLeafRef | leaf record) inside the
-// scene's arrays.
-HPT_HD bool valid_ref(const DevScene& s, int ref) {
-  return ref >= 0 && ((ref & kLeafRef) ? (ref & ~kLeafRef) < s.num_leaves : ref < s.num_nodes);
-}
-
-// Side of a split for the entry point: right when beyond it; a point on
-// the plane follows the direction, and a ray lying in the plane takes the
-// side of the current in-plane walk (tie_goes_right).
-HPT_HD bool goes_right(float p, float split, float dd, TravCold& tc, uint32_t axis) {
-  return p > split || (p == split && (dd > 0.f || (dd == 0.f && tie_goes_right(tc, axis))));
 }
 
 // Node fetch with an optional shared-memory copy of the first n_smem nodes.
@@ -281,39 +262,35 @@ template <bool kUV = false>
 HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint2* smem,
                       int n_smem, DevErr* err, TravCount& cnt) {
   if (st.node < 0) return true;
-  HPT_DCHECK(err, valid_ref(s, st.node), 101, st.node, { st.node = -1; return true; });
+  HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
   const Ray& r = st.ray;
   // Entry point p = o + t_entry * d (kernel.cl:291 style, no FMA).
   const float px = rn_add(r.o.x, rn_mul(st.t_entry, r.d.x));
   const float py = rn_add(r.o.y, rn_mul(st.t_entry, r.d.y));
   const float pz = rn_add(r.o.z, rn_mul(st.t_entry, r.d.z));
   int node = st.node;
-  int leaf_idx;
-  if (node & kLeafRef) {  // a leaf reference: no node load
-    leaf_idx = node & ~kLeafRef;
-  } else {
-    uint2 nd = fetch_node(s, smem, n_smem, node);
-    while ((nd.x >> 30) != kLeafKind) {
-      const uint32_t axis = nd.x >> 30;
-      const float split = as_float_u(nd.y);
-      const float p = axis == 0 ? px : (axis == 1 ? py : pz);
-      const float dd = axis == 0 ? r.d.x : (axis == 1 ? r.d.y : r.d.z);
-      const bool right = goes_right(p, split, dd, tc, axis);
-      HPT_DCHECK(err, (int)(nd.x & kIndexMask) + 1 < s.num_nodes, 106, nd.x & kIndexMask,
-                 { st.node = -1; return true; });
-      node = (int)(nd.x & kIndexMask) + (right ? 1 : 0);
-      nd = fetch_node(s, smem, n_smem, node);
-      ++cnt.nodes;
-      if (++st.steps > s.max_steps) {
-        hpt_atomic_or(&err->flags, 1u);
-        st.node = -1;
-        return true;
-      }
+  uint2 nd = fetch_node(s, smem, n_smem, node);
+  while ((nd.x >> 30) != kLeafKind) {
+    const uint32_t axis = nd.x >> 30;
+    const float split = as_float_u(nd.y);
+    const float p = axis == 0 ? px : (axis == 1 ? py : pz);
+    const float dd = axis == 0 ? r.d.x : (axis == 1 ? r.d.y : r.d.z);
+    const bool right =
+        p > split || (p == split && (dd > 0.f || (dd == 0.f && tie_goes_right(tc, axis))));
+    HPT_DCHECK(err, (int)(nd.x & kIndexMask) + 1 < s.num_nodes, 106, nd.x & kIndexMask,
+               { st.node = -1; return true; });
+    node = (int)(nd.x & kIndexMask) + (right ? 1 : 0);
+    nd = fetch_node(s, smem, n_smem, node);
+    ++cnt.nodes;
+    if (++st.steps > s.max_steps) {
+      hpt_atomic_or(&err->flags, 1u);
+      st.node = -1;
+      return true;
     }
-    leaf_idx = (int)(nd.x & kIndexMask);
   }
-  HPT_DCHECK(err, leaf_idx < s.num_leaves, 102, leaf_idx, { st.node = -1; return true; });
-  const DevLeaf* L = s.leaves + leaf_idx;
+  HPT_DCHECK(err, (int)(nd.x & kIndexMask) < s.num_leaves, 102, nd.x & kIndexMask,
+             { st.node = -1; return true; });
+  const DevLeaf* L = s.leaves + (nd.x & kIndexMask);
   const float4 L0 = ldg(reinterpret_cast<const float4*>(L));
   const float4 L1 = ldg(reinterpret_cast<const float4*>(L) + 1);
   // Exit distance and face (reciprocal multiplies; only the reference's box
@@ -392,7 +369,7 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint
             st.best.u = u;
             st.best.v = v;
           }
-          tc.best_node = kLeafRef | leaf_idx;
+          tc.best_node = node;
         }
       }
     }
@@ -409,7 +386,7 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint
     st.node = -1;
     return true;
   }
-  HPT_DCHECK(err, valid_ref(s, rope), 105, rope, { st.node = -1; return true; });
+  HPT_DCHECK(err, rope < s.num_nodes, 105, rope, { st.node = -1; return true; });
   st.node = rope;
   st.t_entry = fmaxf(st.t_entry, t_exit);
   return false;
@@ -439,36 +416,33 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, TravCold& tc, const uint
   if (st.node < 0) return true;
   const Ray& r = st.ray;
   if (st.phase == kStepDescend) {
-    HPT_DCHECK(err, valid_ref(s, st.node), 101, st.node, { st.node = -1; return true; });
-    int leaf;
-    if (st.node & kLeafRef) {  // a leaf reference: no node load
-      leaf = st.node & ~kLeafRef;
-    } else {
-      const uint2 nd = fetch_node(s, smem, kSmem ? n_smem : 0, st.node);
-      if ((nd.x >> 30) != kLeafKind) {
-        // One descent step; the entry point p = o + t_entry * d on the split
-        // axis (kernel.cl:291 style, no FMA), as trav_leaf computes it.
-        const uint32_t axis = nd.x >> 30;
-        const float split = as_float_u(nd.y);
-        const float o = axis == 0 ? r.o.x : (axis == 1 ? r.o.y : r.o.z);
-        const float dd = axis == 0 ? r.d.x : (axis == 1 ? r.d.y : r.d.z);
-        const float p = rn_add(o, rn_mul(st.t_entry, dd));
-        const bool right = goes_right(p, split, dd, tc, axis);
-        HPT_DCHECK(err, (int)(nd.x & kIndexMask) + 1 < s.num_nodes, 106, nd.x & kIndexMask,
-                   { st.node = -1; return true; });
-        st.node = (int)(nd.x & kIndexMask) + (right ? 1 : 0);
-        ++cnt.nodes;
-        if (++st.steps > s.max_steps) {
-          hpt_atomic_or(&err->flags, 1u);
-          st.node = -1;
-          return true;
-        }
-        return false;
+    HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
+    const uint2 nd = fetch_node(s, smem, kSmem ? n_smem : 0, st.node);
+    if ((nd.x >> 30) != kLeafKind) {
+      // One descent step; the entry point p = o + t_entry * d on the split
+      // axis (kernel.cl:291 style, no FMA), as trav_leaf computes it.
+      const uint32_t axis = nd.x >> 30;
+      const float split = as_float_u(nd.y);
+      const float o = axis == 0 ? r.o.x : (axis == 1 ? r.o.y : r.o.z);
+      const float dd = axis == 0 ? r.d.x : (axis == 1 ? r.d.y : r.d.z);
+      const float p = rn_add(o, rn_mul(st.t_entry, dd));
+      const bool right =
+        p > split || (p == split && (dd > 0.f || (dd == 0.f && tie_goes_right(tc, axis))));
+      HPT_DCHECK(err, (int)(nd.x & kIndexMask) + 1 < s.num_nodes, 106, nd.x & kIndexMask,
+                 { st.node = -1; return true; });
+      st.node = (int)(nd.x & kIndexMask) + (right ? 1 : 0);
+      ++cnt.nodes;
+      if (++st.steps > s.max_steps) {
+        hpt_atomic_or(&err->flags, 1u);
+        st.node = -1;
+        return true;
       }
-      leaf = (int)(nd.x & kIndexMask);
+      return false;
     }
     // Leaf set-up: exit distance and face, triangle range.
-    HPT_DCHECK(err, leaf < s.num_leaves, 102, leaf, { st.node = -1; return true; });
+    HPT_DCHECK(err, (int)(nd.x & kIndexMask) < s.num_leaves, 102, nd.x & kIndexMask,
+               { st.node = -1; return true; });
+    const int leaf = (int)(nd.x & kIndexMask);
     const float4* L = reinterpret_cast<const float4*>(s.leaves + leaf);
     // The six ropes are read with the box (independent loads) so that the
     // exit needs no dependent load of its own.
@@ -504,7 +478,7 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, TravCold& tc, const uint
     st.k = begin;
     st.end = begin + count;
     tc.leaf = leaf;
-    tc.leaf_node = kLeafRef | leaf;
+    tc.leaf_node = st.node;
     tc.rope = face == 0 ? R03.x : face == 1 ? R03.y : face == 2 ? R03.z
             : face == 3 ? R03.w : face == 4 ? R45.x : face == 5 ? R45.y : -1;
     tc.t_exit = t_exit;
@@ -581,7 +555,7 @@ HPT_HD bool trav_step(const DevScene& s, TravState& st, TravCold& tc, const uint
     st.node = -1;
     return true;
   }
-  HPT_DCHECK(err, valid_ref(s, rope), 105, rope, { st.node = -1; return true; });
+  HPT_DCHECK(err, rope < s.num_nodes, 105, rope, { st.node = -1; return true; });
   st.node = rope;
   st.t_entry = fmaxf(st.t_entry, tc.t_exit);
   return false;

@@ -108,11 +108,16 @@ def test_cornell_readme_render_matches_counter_oracle(cornell):
 def test_cornell_image_vs_reference_kernels(cornell):
     """The GPU's estimate (1024 spp) against the reference kernels' own
     estimate stored in the fixture (256 spp, same camera and depth).
-    Calibration: two runs of the reference estimator (1024 vs 256 spp) put
-    94.1 % of ray means within 3 sigma, relMSE 1.32x the value the
-    per-sample variances predict, totals 0.2 % apart; the counter-mode
-    oracle (the GPU's streams) gives 93.8 %, 1.37x, 0.2 %. Bars: >= 90 %,
-    relMSE <= 1.6x predicted, totals within 1 %."""
+    At this scale the reference's image depends on the last bits of its
+    math library: a next ray that starts on the surface it left re-hits it
+    or not according to those bits. Two runs of the reference estimator
+    (1024 vs 256 spp) put 94.1 % of ray means within 3 sigma, relMSE 1.32x
+    the value the per-sample variances predict, totals 0.2 % apart; the
+    oracle with every acos / asin / sin / cos / pow result moved one ulp
+    toward zero (an equally valid library) gives relMSE 12.3x, totals
+    0.3-0.4 %. CUDA's library is another such library. Bars: >= 90 % within
+    3 sigma, relMSE below the one-ulp library's 12.3x, totals within 1 %.
+    The unit-scale copy of the box below carries the tight bars."""
     f, cam, gpu, _ = cornell
     w, spp_o, depth = int(f["res"]), int(f["spp"]), int(f["depth"])
     spp_g = 1024
@@ -129,6 +134,73 @@ def test_cornell_image_vs_reference_kernels(cornell):
     print("Cornell vs reference kernels: within 3 sigma %.4f, relMSE %.4g (predicted %.4g), "
           "totals %.4g" % (frac, relmse, expected, total))
     assert frac >= 0.90
+    assert relmse <= 12.3 * expected
+    assert total < 0.01
+
+
+@pytest.fixture(scope="module")
+def cornell_unit(built):
+    """The same box scaled by 1/556 (one unit across): the reference's 1e-5
+    origin offset is far above an ulp there, so paths are not chaotic (a
+    one-ulp camera move changes 0.27 % of the oracle's rays, against 37 %
+    at full scale). The KD-tree is rebuilt by the SAH builder, which gives
+    the reference builder's tree bit for bit."""
+    if H.device_count() == 0:
+        pytest.skip("no CUDA device")
+    f = dict(np.load(GOLD))
+    k = np.float32(1.0 / 556.0)
+    pts = f["points"].copy()
+    pts[:, :3] *= k
+    mesh = H.Mesh(pts, f["triangles"], f["materials"], f["normals"], f["texcoords"])
+    mesh.rebuild_lights()
+    nodes, leaf = H.build_kdtree(mesh.points, mesh.triangles)
+    c = f["camera"]
+    cam = dict(view_p=tuple(float(np.float32(x) * k) for x in c[0:3]),
+               top_dir=tuple(float(x) for x in c[3:6]), right_dir=tuple(float(x) for x in c[6:9]),
+               width=float(c[9]), height=float(c[10]))
+    return cam, H.Scene(mesh, nodes, leaf), O.CpuScene(mesh, nodes, leaf)
+
+
+def test_cornell_unit_scale_matches_counter_oracle(cornell_unit):
+    """Readme settings (50 spp, depth 5), 100 x 100: per-ray radiance against
+    the oracle driven by the GPU's random streams: <= 2 % of rays off by
+    more than 1e-3, totals and query counts within 1 %."""
+    cam, gpu, cpu = cornell_unit
+    p = H.make_params(100, 100, 1, 1, (0, 0, 0), 50, 5, 0, 1.0, 50)
+    _, acc = gpu.render(_hp(cam), p, want_accum=True)
+    st = gpu.stats()
+    ref, _, counts = cpu.render(cam, 100, 100, 1, 1, (0, 0, 0), 50, 5, 0, seed=50, rng_mode=1,
+                                threads=THREADS)
+    bad = _off(acc, ref)
+    print("Cornell unit scale: rays off by >1e-3: %.4f; queries gpu %d oracle %d"
+          % (bad, st["intersect_queries"], counts[0]))
+    assert bad < 0.02
+    assert abs(acc.sum() - ref.sum()) / ref.sum() < 0.01
+    assert abs(st["intersect_queries"] - counts[0]) / counts[0] < 0.01
+    assert st["error_flags"] == 0
+
+
+def test_cornell_unit_scale_vs_reference_estimator(cornell_unit):
+    """GPU 1024 spp against the reference's own estimator (per-lane LCG,
+    256 spp, computed here). Calibration on this scene: the counter-mode
+    oracle and a second reference run give 97.3-97.4 % within 3 sigma,
+    relMSE 1.38-1.41x predicted, totals 0.2-0.3 % apart. Bars: >= 95 %,
+    relMSE <= 1.6x predicted, totals within 1 %."""
+    cam, gpu, cpu = cornell_unit
+    p = H.make_params(100, 100, 1, 1, (0, 0, 0), 1024, 5, 0, 1.0, 3)
+    _, acc = gpu.render(_hp(cam), p, want_accum=True)
+    ref, ref2, _ = cpu.render(cam, 100, 100, 1, 1, (0, 0, 0), 256, 5, 0, seed=9, rng_mode=0,
+                              threads=THREADS)
+    mg, mo = acc / 1024, ref / 256
+    var = np.maximum(ref2 / 256 - mo * mo, 0.0)
+    sigma = np.sqrt(var / 1024 + var / 256) + 1e-5 * np.abs(mo) + 1e-6
+    frac = (np.abs(mg - mo) / sigma <= 3).mean()
+    relmse = np.mean((mg - mo) ** 2 / (mo ** 2 + 1e-2))
+    expected = np.mean((var / 1024 + var / 256) / (mo ** 2 + 1e-2))
+    total = abs(mg.sum() - mo.sum()) / mo.sum()
+    print("Cornell unit scale vs reference estimator: within 3 sigma %.4f, relMSE %.4g "
+          "(predicted %.4g), totals %.4g" % (frac, relmse, expected, total))
+    assert frac >= 0.95
     assert relmse <= 1.6 * expected
     assert total < 0.01
 

@@ -155,8 +155,7 @@ def test_bad_hints_fall_back_to_root(pair):
 def test_packed_tree_structure(pair):
     """Children sit side by side, every leaf record's ref range is inside
     leaf_refs, and every rope names a node of the tree (the smallest one that
-    covers that face, Popov et al. 2007; a leaf by its record) or -1 on the
-    scene boundary."""
+    covers that face, Popov et al. 2007) or -1 on the scene boundary."""
     cs, em = pair
     c = em.counts()
     meta, split, leaves = em.tree()
@@ -171,13 +170,8 @@ def test_packed_tree_structure(pair):
     first, count = leaves[:, 3], leaves[:, 7]
     assert ((first >= 0) & (count >= 0) & (first + count <= c["refs"])).all()
     ropes = leaves[:, 8:14]
-    # A rope is -1 on the scene boundary, a node index, or (when the
-    # smallest node covering the face is a leaf) that leaf's record tagged
-    # with bit 30.
-    is_leaf = (ropes >= 0) & ((ropes & (1 << 30)) != 0)
-    assert ((ropes == -1) | ((ropes > 0) & (ropes < c["nodes"])) |
-            (is_leaf & ((ropes & ~(1 << 30)) < c["leaves"]))).all()
-    assert (ropes >= 0).any() and is_leaf.any()
+    assert ((ropes == -1) | ((ropes > 0) & (ropes < c["nodes"]))).all()
+    assert (ropes >= 0).any()
 
 
 def test_shade_and_next_dir_match_oracle(pair):
