@@ -84,6 +84,22 @@ struct DevScene {
   int32_t max_steps;        // traversal step cap per ray
 };
 
+// The fields of a DevScene the traversal reads (80 bytes): a launch whose
+// jobs render several scenes keeps one per job slot in shared memory, so a
+// traversal step reads its scene's pointers and sizes from there instead
+// of from the job table in global memory.
+struct TravScene {
+  const DevNode* nodes;
+  const DevLeaf* leaves;
+  const int32_t* leaf_refs;
+  const DevTri* tris;
+  int32_t num_nodes, num_leaves, num_leaf_tris, num_triangles;
+  float root_lo[3], root_hi[3];
+  float scene_eps;
+  int32_t max_steps;
+};
+static_assert(sizeof(TravScene) == 80, "80-byte traversal scene");
+
 // --- Wavefront job table ------------------------------------------------
 // One render job (a frame of one scene) in a slot of the engine's table.
 // Read-only while the job runs; its mutable scheduling state is DevSlot.

@@ -77,6 +77,9 @@ struct EngineParams {
   // traversal unit (one dependent load less per unit).
   int uniform_scene;
   DevScene uscene;
+  // Several scenes, and their per-slot TravScene table fits the dynamic
+  // shared memory: the traversal reads its scene from there.
+  int scene_table;
 };
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -175,6 +178,18 @@ __device__ __forceinline__ int stage_nodes(const EngineParams& P, uint2* snodes)
   return P.smem_nodes;
 }
 
+// A launch over several scenes copies each job slot's TravScene into the
+// dynamic shared memory (the node prefix is only used by one-scene
+// launches, so the table starts at offset 0): the traversal steps then read
+// their scene's pointers and sizes from shared memory.
+__device__ __forceinline__ const TravScene* stage_scenes(const EngineParams& P, uint2* smem) {
+  if (!P.scene_table) return nullptr;
+  TravScene* tab = reinterpret_cast<TravScene*>(smem);
+  for (int i = threadIdx.x; i < P.num_slots; i += blockDim.x) tab[i] = trav_scene(P.jobs[i].scene);
+  __syncthreads();
+  return tab;
+}
+
 // Grants the free wavefront capacity to active slots in priority order
 // (one thread). A slot with nothing left to issue no longer needs grants.
 __device__ void schedule(const EngineParams& P) {
@@ -237,6 +252,7 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
   constexpr bool kStep = kMode != kTravLeaf;
   extern __shared__ uint2 snodes[];
   const int n_smem = kMode == kTravStep ? 0 : stage_nodes(P, snodes);
+  const TravScene* scene_tab = stage_scenes(P, snodes);
   DevCtrl* c = P.ctrl;
   const int lane = threadIdx.x & 31;
   const int64_t total = P.prim_prefix[P.prim_n];
@@ -290,6 +306,14 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
           for (int u = 0; u < P.trav_steps; ++u)
             if (trav_step<false, kMode == kTravStepSmem>(P.uscene, st, tc, snodes, n_smem,
                                                          &c->err, cnt)) {
+              finished = true;
+              break;
+            }
+        } else if (P.scene_table) {
+          const TravScene& sc = scene_tab[slot];
+          for (int u = 0; u < P.trav_steps; ++u)
+            if (trav_step<false, kMode == kTravStepSmem>(sc, st, tc, snodes, n_smem, &c->err,
+                                                         cnt)) {
               finished = true;
               break;
             }
@@ -514,6 +538,7 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
   constexpr bool kStep = kMode != kTravLeaf;
   extern __shared__ uint2 snodes[];
   const int n_smem = kMode == kTravStep ? 0 : stage_nodes(P, snodes);
+  const TravScene* scene_tab = stage_scenes(P, snodes);
   DevCtrl* c = P.ctrl;
   const int n = c->nR;
   const int out_par = c->parity ^ 1;
@@ -565,6 +590,14 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
           for (int u = 0; u < P.trav_steps; ++u)
             if (trav_step<false, kMode == kTravStepSmem>(P.uscene, st, tc, snodes, n_smem,
                                                          &c->err, cnt)) {
+              finished = true;
+              break;
+            }
+        } else if (P.scene_table) {
+          const TravScene& sc = scene_tab[slot];
+          for (int u = 0; u < P.trav_steps; ++u)
+            if (trav_step<false, kMode == kTravStepSmem>(sc, st, tc, snodes, n_smem, &c->err,
+                                                         cnt)) {
               finished = true;
               break;
             }
@@ -1085,6 +1118,10 @@ DevJob Engine::make_job(const JobSpec& js, const JobBuffers& b) const {
   return j;
 }
 
+// Largest per-slot scene table kept in shared memory (102 slots): 10
+// blocks of 128 per SM then still fit beside their static shared memory.
+constexpr size_t kSceneTableBytes = 8192;
+
 static EngineParams make_params(const Engine& e, DevCtrl* ctrl, DevJob* jobs, DevSlot* slots,
                                 int num_slots, const int32_t* order, int32_t* quota_slot,
                                 int32_t* quota_prefix, const int32_t* prim_slot,
@@ -1126,7 +1163,15 @@ static EngineParams make_params(const Engine& e, DevCtrl* ctrl, DevJob* jobs, De
     P.smem_nodes = std::min(e.tuning.smem_nodes, shared->num_nodes);
     P.shared_nodes = shared->nodes;
   }
+  if (!shared && (size_t)num_slots * sizeof(TravScene) <= kSceneTableBytes) P.scene_table = 1;
   return P;
+}
+
+// Dynamic shared memory of a traversal launch: the node prefix of a
+// one-scene launch, or the per-slot scene table of a several-scene one.
+static size_t launch_smem(const EngineParams& P) {
+  return P.scene_table ? (size_t)P.num_slots * sizeof(TravScene)
+                       : (size_t)P.smem_nodes * sizeof(uint2);
 }
 
 void Engine::reset_ctrl() {
@@ -1182,7 +1227,7 @@ hpt_status Engine::admit(const std::vector<int>& slot_ids, const std::vector<Dev
   EngineParams P = make_params(*this, ctrl_, jobs_, slot_state_, slots_, order_, quota_slot_,
                                quota_prefix_, prim_slot_, prim_prefix_, n, capacity_, A, A_tri_,
                                A_leaf_, R, shared_scene);
-  const size_t smem = (size_t)P.smem_nodes * sizeof(uint2);
+  const size_t smem = launch_smem(P);
   const IsectVariant& v = kIsectVariants[isect_variant()];
   v.primary_kernel(P.trav_steps, P.smem_nodes)<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
   HPT_CUDA(cudaGetLastError());
@@ -1281,7 +1326,7 @@ hpt_status Engine::admit_async(const std::vector<int>& slot_ids, const std::vect
   EngineParams P = make_params(*this, ctrl_, jobs_, slot_state_, slots_, order_, quota_slot_,
                                quota_prefix_, prim_slot_, prim_prefix_, n, capacity_, A, A_tri_,
                                A_leaf_, R, shared_scene);
-  const size_t smem = (size_t)P.smem_nodes * sizeof(uint2);
+  const size_t smem = launch_smem(P);
   const IsectVariant& v = kIsectVariants[isect_variant()];
   v.primary_kernel(P.trav_steps, P.smem_nodes)<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
   k_admit<<<1, 1, 0, stream>>>(P);
@@ -1352,7 +1397,7 @@ void Engine::launch_iteration(const DevScene* shared_scene, cudaEvent_t* ev) {
   if (ev) HPT_SOFT(cudaEventRecord(ev[0], stream));
   shade_kernel(tuning)<<<num_sms * occ_shade_, 256, 0, stream>>>(P);
   if (ev) HPT_SOFT(cudaEventRecord(ev[1], stream));
-  const size_t smem = (size_t)P.smem_nodes * sizeof(uint2);
+  const size_t smem = launch_smem(P);
   const IsectVariant& v = kIsectVariants[isect_variant()];
   v.isect_kernel(P.trav_steps, P.smem_nodes)<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);
   if (ev) HPT_SOFT(cudaEventRecord(ev[2], stream));

@@ -175,7 +175,8 @@ struct TravCount {
 // Starts a query. start_node (>= 0) names a leaf node the origin is
 // expected to lie in (the leaf of the previous hit): if its box contains the
 // origin the walk starts there instead of descending from the root.
-HPT_HD void trav_init(const DevScene& s, const Ray& r, TravState& st, TravCold& tc,
+template <class Sc>
+HPT_HD void trav_init(const Sc& s, const Ray& r, TravState& st, TravCold& tc,
                       int start_node = -1) {
   st.ray = r;
   st.best.rec = -1;
@@ -244,8 +245,29 @@ HPT_HD void trav_init(const DevScene& s, const Ray& r, TravState& st, TravCold& 
   }
 }
 
+// The traversal's view of a scene (the fields trav_* read).
+HPT_HD TravScene trav_scene(const DevScene& s) {
+  TravScene t;
+  t.nodes = s.nodes;
+  t.leaves = s.leaves;
+  t.leaf_refs = s.leaf_refs;
+  t.tris = s.tris;
+  t.num_nodes = s.num_nodes;
+  t.num_leaves = s.num_leaves;
+  t.num_leaf_tris = s.num_leaf_tris;
+  t.num_triangles = s.num_triangles;
+  for (int a = 0; a < 3; ++a) {
+    t.root_lo[a] = s.root_lo[a];
+    t.root_hi[a] = s.root_hi[a];
+  }
+  t.scene_eps = s.scene_eps;
+  t.max_steps = s.max_steps;
+  return t;
+}
+
 // Node fetch with an optional shared-memory copy of the first n_smem nodes.
-HPT_HD uint2 fetch_node(const DevScene& s, const uint2* smem, int n_smem,
+template <class Sc>
+HPT_HD uint2 fetch_node(const Sc& s, const uint2* smem, int n_smem,
                                             int i) {
   if (i < n_smem) return smem[i];
   return ldg(reinterpret_cast<const uint2*>(s.nodes) + i);
@@ -258,8 +280,8 @@ constexpr uint32_t kDeadLeafMeta = 0xFFFFFFFFu;
 // entry point, tests its triangles, then follows the exit rope.
 // Returns true when the ray is finished.
 // kUV: also report the winning test's Moller-Trumbore u, v (stage entry).
-template <bool kUV = false>
-HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint2* smem,
+template <bool kUV = false, class Sc = DevScene>
+HPT_HD bool trav_leaf(const Sc& s, TravState& st, TravCold& tc, const uint2* smem,
                       int n_smem, DevErr* err, TravCount& cnt) {
   if (st.node < 0) return true;
   HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
@@ -410,8 +432,8 @@ HPT_HD bool trav_leaf(const DevScene& s, TravState& st, TravCold& tc, const uint
 // Returns true when the ray is finished.
 // kSmem: nodes below n_smem are read from the shared-memory prefix (false:
 // every node from global memory, and smem / n_smem are ignored).
-template <bool kUV = false, bool kSmem = true>
-HPT_HD bool trav_step(const DevScene& s, TravState& st, TravCold& tc, const uint2* smem,
+template <bool kUV = false, bool kSmem = true, class Sc = DevScene>
+HPT_HD bool trav_step(const Sc& s, TravState& st, TravCold& tc, const uint2* smem,
                       int n_smem, DevErr* err, TravCount& cnt) {
   if (st.node < 0) return true;
   const Ray& r = st.ray;
