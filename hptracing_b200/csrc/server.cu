@@ -76,6 +76,7 @@ struct Request {
   int64_t done_paths = 0;
   int64_t queries = 0;
   double submit_ms = 0, admit_ms = 0, done_ms = 0;
+  double due_ms = -1;       // completion the overload policy predicted at admission
   hpt_status error = HPT_OK;
   uint8_t* rgba = nullptr;  // pinned, from the server's pool
   float* accum = nullptr;
@@ -122,6 +123,10 @@ struct hpt_server {
   // the first-come first-served line), smoothed; -1 = not measured yet.
   std::vector<double> svc_ms;
   double last_small_done_ms = 0;
+  // How much later than predicted latency-bound requests finish (read-back
+  // and resolve latency, and the spread of service times): a high quantile
+  // tracked with an asymmetric running average (quick to rise, slow to fall).
+  double late_ms = 0;
   int64_t shed = 0;
 
   double now_ms() const {
@@ -236,12 +241,15 @@ hpt_status hpt_server::admit_pending() {
         continue;
       }
       const double svc = service_estimate(r->scene_slot);
-      if (small_waiting || (svc >= 0 && waited + backlog + svc > cfg.deadline_ms)) {
+      if (small_waiting || (svc >= 0 && waited + backlog + svc + late_ms > cfg.deadline_ms)) {
         small_waiting = true;  // later latency-bound requests wait behind it
         ++it;
         continue;
       }
-      if (svc >= 0) backlog += svc;
+      if (svc >= 0) {
+        backlog += svc;
+        r->due_ms = now + backlog;
+      }
     }
     int slot = -1;
     for (size_t k = 0; k < slot_req.size(); ++k)
@@ -366,6 +374,10 @@ hpt_status hpt_server::retire_finished() {
       if ((int)svc_ms.size() <= r->scene_slot) svc_ms.resize(r->scene_slot + 1, -1.0);
       double& e = svc_ms[r->scene_slot];
       e = e < 0 ? dt : 0.7 * e + 0.3 * dt;
+      if (r->due_ms >= 0) {
+        const double late = std::max(0.0, r->done_ms - r->due_ms);
+        late_ms += (late > late_ms ? 0.3 : 0.02) * (late - late_ms);
+      }
     }
   }
   return HPT_OK;
