@@ -710,9 +710,10 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, duration, capacity, la
         "requests": len(arrivals), "completed": len(lat["pose"]) + len(lat["pano"]),
         "shed": shed,
         "policy": {"deadline_ms": deadline_ms,
-                   "rule": ("requests of <= capacity paths first-come first-served ahead of "
-                            "larger ones, admitted while the admitted ones are expected to "
-                            "finish within the deadline, shed when still queued past it")
+                   "rule": ("requests of <= capacity paths granted first-come first-served "
+                            "ahead of larger ones; each admitted when predicted to finish "
+                            "within the deadline behind those admitted, shed once it could "
+                            "not finish in time on an idle wavefront")
                    if deadline_ms > 0 else "smallest remaining work first, no shedding"},
         "unfinished": len(outstanding) + (len(arrivals) - nxt),
         "pose_512x512_4spp": {"n": len(lat["pose"]), "p50_ms": pct(lat["pose"], 50),

@@ -77,6 +77,8 @@ struct Request {
   int64_t queries = 0;
   double submit_ms = 0, admit_ms = 0, done_ms = 0;
   double due_ms = -1;       // completion the overload policy predicted at admission
+  bool alone = false;       // admitted while no other latency-bound request ran
+  double drift_ms = 0;      // the server's prediction drift when it was admitted
   hpt_status error = HPT_OK;
   uint8_t* rgba = nullptr;  // pinned, from the server's pool
   float* accum = nullptr;
@@ -117,16 +119,20 @@ struct hpt_server {
   std::vector<cudaEvent_t> event_pool;
   int64_t completed = 0;
   int64_t pumps = 0;
-  // Overload policy (cfg.deadline_ms > 0): per-scene service time of a
-  // latency-bound request (its completion minus the later of its admission
-  // and the previous latency-bound completion, i.e. its time at the head of
-  // the first-come first-served line), smoothed; -1 = not measured yet.
-  std::vector<double> svc_ms;
+  // Overload policy (cfg.deadline_ms > 0). Per scene, two service times of
+  // a latency-bound request, each an upper quantile of recent observations:
+  // `alone` = completion minus admission for one admitted while no other
+  // latency-bound request was running, `gap` = completion minus the previous
+  // latency-bound completion for one admitted behind others. -1 = not
+  // measured yet.
+  struct ServiceEstimate {
+    double alone = -1, gap = -1;
+    bool probing = false;  // the first request of the scene is running
+  };
+  std::vector<ServiceEstimate> est;
   double last_small_done_ms = 0;
-  // How much later than predicted latency-bound requests finish (read-back
-  // and resolve latency, and the spread of service times): a high quantile
-  // tracked with an asymmetric running average (quick to rise, slow to fall).
-  double late_ms = 0;
+  double tail_ms = 0;  // predicted completion of the latest admitted latency-bound request
+  double drift_ms = 0;  // sum of the corrections applied to the predictions so far
   int64_t shed = 0;
 
   double now_ms() const {
@@ -163,22 +169,15 @@ struct hpt_server {
     for (auto& p : v) o.push_back(p.second);
     return o;
   }
-  double service_estimate(int scene) const {
-    return scene < (int)svc_ms.size() ? svc_ms[scene] : -1.0;
+  ServiceEstimate& estimate(int scene) {
+    if ((int)est.size() <= scene) est.resize(scene + 1);
+    return est[scene];
   }
-  // Expected time until the latency-bound requests already admitted finish.
-  double small_backlog_ms() const {
-    double ms = 0;
-    for (size_t k = 0; k < slot_req.size(); ++k) {
-      if (!slot_req[k]) continue;
-      const Request* r = reqs.at(slot_req[k]).get();
-      if (!r->small || r->finishing) continue;
-      const double svc = service_estimate(r->scene_slot);
-      if (svc < 0) continue;
-      const double left = r->paths > 0 ? 1.0 - (double)r->done_paths / (double)r->paths : 1.0;
-      ms += svc * std::max(0.0, left);
-    }
-    return ms;
+  // Latency-bound requests admitted and not yet retired.
+  bool small_running() const {
+    for (size_t k = 0; k < slot_req.size(); ++k)
+      if (slot_req[k] && reqs.at(slot_req[k])->small) return true;
+    return false;
   }
   hpt_status take_pinned(size_t bytes, void** out) {
     auto it = pinned_pool.find(bytes);
@@ -215,8 +214,7 @@ hpt_status hpt_server::admit_pending() {
   std::vector<DevJob> jobs;
   std::vector<int64_t> rays;
   const double now = now_ms();
-  double backlog = cfg.deadline_ms > 0 ? small_backlog_ms() : 0.0;
-  bool small_waiting = false;
+  bool busy = cfg.deadline_ms > 0 && small_running();
   for (auto it = queue.begin(); it != queue.end();) {
     Request* r = find(*it);
     if (!r || r->cancel) {
@@ -227,12 +225,19 @@ hpt_status hpt_server::admit_pending() {
       it = queue.erase(it);
       continue;
     }
+    double due = -1;
     if (cfg.deadline_ms > 0 && r->small) {
-      // Overload policy: shed what can no longer meet its deadline; admit
-      // first-come first-served only while the admitted latency-bound work
-      // plus this request is expected to finish in time.
+      // Overload policy. A request that cannot finish within the deadline
+      // even on an idle wavefront is shed now; one that would finish in time
+      // behind the latency-bound work already admitted is admitted; the rest
+      // wait (without holding back younger requests that fit) until they
+      // fit or are shed.
       const double waited = now - r->submit_ms;
-      if (waited > cfg.deadline_ms) {
+      ServiceEstimate& e = estimate(r->scene_slot);
+      if (waited > cfg.deadline_ms || (e.alone >= 0 && waited + e.alone > cfg.deadline_ms)) {
+        // A stale estimate would shed this scene's requests for good:
+        // every shed lowers it a little so that one is measured again.
+        if (e.alone >= 0) e.alone *= 0.98;
         r->state = kCancelled;
         r->shed = true;
         ++shed;
@@ -240,15 +245,16 @@ hpt_status hpt_server::admit_pending() {
         it = queue.erase(it);
         continue;
       }
-      const double svc = service_estimate(r->scene_slot);
-      if (small_waiting || (svc >= 0 && waited + backlog + svc + late_ms > cfg.deadline_ms)) {
-        small_waiting = true;  // later latency-bound requests wait behind it
-        ++it;
+      if (e.alone >= 0) {
+        due = now + e.alone;
+        if (busy) due = std::max(due, tail_ms + (e.gap >= 0 ? e.gap : e.alone));
+        if (due - r->submit_ms > cfg.deadline_ms) {
+          ++it;
+          continue;
+        }
+      } else if (e.probing) {
+        ++it;  // one request measures a new scene before more are admitted
         continue;
-      }
-      if (svc >= 0) {
-        backlog += svc;
-        r->due_ms = now + backlog;
       }
     }
     int slot = -1;
@@ -274,6 +280,14 @@ hpt_status hpt_server::admit_pending() {
     r->state = kRunning;
     r->admit_ms = now_ms();
     r->admit_seq = launched;
+    if (cfg.deadline_ms > 0 && r->small) {
+      r->due_ms = due;
+      r->drift_ms = drift_ms;
+      r->alone = !busy;
+      if (due >= 0) tail_ms = busy ? std::max(tail_ms, due) : due;
+      if (due < 0) estimate(r->scene_slot).probing = true;
+      busy = true;
+    }
     slot_req[slot] = r->id;
     used_bytes += r->footprint;
     ids.push_back(slot);
@@ -367,16 +381,25 @@ hpt_status hpt_server::retire_finished() {
     r->done_ms = now_ms();
     finished_ids.push_back(r->id);
     ++completed;
-    if (r->small && !r->cancel) {
-      const double head = std::max(r->admit_ms, last_small_done_ms);
-      const double dt = r->done_ms - head;
+    if (r->small && cfg.deadline_ms > 0) estimate(r->scene_slot).probing = false;
+    if (r->small && !r->cancel && cfg.deadline_ms > 0) {
+      // Upper-quantile running estimates: quick to rise, slow to fall.
+      auto track = [](double& q, double x) {
+        q = q < 0 ? x : q + (x > q ? 0.25 : 0.05) * (x - q);
+      };
+      ServiceEstimate& e = estimate(r->scene_slot);
+      if (r->alone || e.alone < 0)
+        track(e.alone, r->done_ms - r->admit_ms);
+      else
+        track(e.gap, r->done_ms - std::max(r->admit_ms, last_small_done_ms));
       last_small_done_ms = r->done_ms;
-      if ((int)svc_ms.size() <= r->scene_slot) svc_ms.resize(r->scene_slot + 1, -1.0);
-      double& e = svc_ms[r->scene_slot];
-      e = e < 0 ? dt : 0.7 * e + 0.3 * dt;
+      // Requests admitted behind this one finish as much earlier or later
+      // than predicted as it did (its prediction already moved by the
+      // corrections made since its admission).
       if (r->due_ms >= 0) {
-        const double late = std::max(0.0, r->done_ms - r->due_ms);
-        late_ms += (late > late_ms ? 0.3 : 0.02) * (late - late_ms);
+        const double delta = r->done_ms - (r->due_ms + drift_ms - r->drift_ms);
+        drift_ms += delta;
+        tail_ms = std::max(r->done_ms, tail_ms + delta);
       }
     }
   }

@@ -418,12 +418,14 @@ typedef struct hpt_server_config {
    * (costs 12 bytes per ray of device memory and copy-back). */
   int32_t keep_accum;
   /* Overload policy (0 = off). Requests with at most `capacity` paths
-   * (rays x spp) are latency-bound: they are served first-come first-served
-   * ahead of larger ones, admitted only while the latency-bound work
-   * already admitted is expected to finish within deadline_ms (per-scene
-   * service times learned from finished requests), and shed when still
-   * queued deadline_ms after submission (poll returns HPT_ERR_CANCELLED;
-   * hpt_server_shed counts them). */
+   * (rays x spp) are latency-bound: they are granted wavefront capacity
+   * first-come first-served ahead of larger ones. Each is admitted when it
+   * is predicted to finish within deadline_ms of its submission behind the
+   * latency-bound work already admitted (per-scene service times learned
+   * from finished requests), waits while it is not, and is shed as soon as
+   * it could not finish in time even on an idle wavefront (poll returns
+   * HPT_ERR_CANCELLED; hpt_server_shed counts them). Larger requests are
+   * never shed. */
   int32_t deadline_ms;
 } hpt_server_config;
 

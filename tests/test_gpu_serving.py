@@ -205,13 +205,13 @@ def test_autotune_picks_a_valid_tuning_and_caches_it(scenes):
 
 
 def test_overload_policy_sheds_late_requests_and_keeps_results(scenes):
-    """deadline_ms: latency-bound requests (<= capacity paths) are served
-    first-come first-served, admitted while the admitted ones are expected
-    to finish in time and shed when still queued past the deadline. A burst
-    of 64 requests with a 1 ms deadline: the first ones run (no service
-    estimate yet), later ones are shed (HPT_ERR_CANCELLED, counted by
-    hpt_server_shed), and every request that does complete is bit-identical
-    to the same request rendered alone. Without the policy nothing is shed."""
+    """deadline_ms: latency-bound requests (<= capacity paths) are admitted
+    when predicted to finish in time and shed once they cannot. A burst of
+    64 requests with a 1 ms deadline: the first runs (it measures the
+    scene's service time), the others are shed (HPT_ERR_CANCELLED, counted
+    by hpt_server_shed), and every request that does complete is
+    bit-identical to the same request rendered alone. Without the policy
+    nothing is shed."""
     req = (1, S.ROOM_CAM, 96, 64, 1, 4, 6, (0, 0, 0), 300)
     _, ref = _alone(scenes, req)
     for deadline, expect_shed in ((1, True), (0, False)):
