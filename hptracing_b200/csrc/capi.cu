@@ -163,8 +163,10 @@ __global__ void k_stage_resolve(const float* accum, int W, int H, int ssx, int s
 // --- Stream compaction: per-tile counts, one scan, stable scatter. -------
 // A tile is 2048 flags: 256 threads x 8 consecutive flags, read as two
 // 16-byte loads where the flag array is 16-byte aligned and the tile is
-// whole. No kernel waits on another block: the three passes are ordered by
-// the stream alone.
+// whole. The flags are read once: the count pass also stores each thread's
+// 8 flags as one mask byte (n / 8 bytes in all), which the scatter pass
+// reads instead of the flags. No kernel waits on another block: the three
+// passes are ordered by the stream alone.
 constexpr int kCompactThreads = 256;
 constexpr int kCompactItems = 8;
 constexpr int kCompactTile = kCompactThreads * kCompactItems;
@@ -216,11 +218,14 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
 }
 
 __global__ void __launch_bounds__(kCompactThreads) k_compact_count(const uint32_t* flags, int n,
-                                                                   int* block_counts) {
+                                                                   int* block_counts,
+                                                                   uint8_t* masks) {
   __shared__ int warp_sum[kCompactThreads / 32];
   const bool vec = (reinterpret_cast<uintptr_t>(flags) & 15) == 0;
   const int64_t i0 = (int64_t)blockIdx.x * kCompactTile + (int64_t)threadIdx.x * kCompactItems;
-  const int c = __popc(load_flags8(flags, i0, n, vec));
+  const uint32_t m = load_flags8(flags, i0, n, vec);
+  masks[(int64_t)blockIdx.x * kCompactThreads + threadIdx.x] = (uint8_t)m;
+  const int c = __popc(m);
   const int w = __reduce_add_sync(0xFFFFFFFFu, c);
   if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = w;
   __syncthreads();
@@ -260,15 +265,16 @@ __global__ void __launch_bounds__(kScanThreads) k_compact_scan(int* counts, int 
   if (threadIdx.x == 0) *total = carry;
 }
 
-__global__ void __launch_bounds__(kCompactThreads) k_compact_scatter(const uint32_t* flags, int n,
+// Mask bytes of flags at or past n are zero (the count pass bounds-checks),
+// so the scatter needs no n.
+__global__ void __launch_bounds__(kCompactThreads) k_compact_scatter(const uint8_t* masks,
                                                                      const int* block_offsets,
                                                                      int* out) {
   __shared__ int staged[kCompactTile];
   __shared__ int tile_count;
-  const bool vec = (reinterpret_cast<uintptr_t>(flags) & 15) == 0;
   const int64_t tile = (int64_t)blockIdx.x * kCompactTile;
   const int64_t i0 = tile + (int64_t)threadIdx.x * kCompactItems;
-  uint32_t m = load_flags8(flags, i0, n, vec);
+  uint32_t m = masks[(int64_t)blockIdx.x * kCompactThreads + threadIdx.x];
   int pos = block_exclusive_scan<kCompactThreads>(__popc(m), &tile_count);
   // Survivor indices of the tile in order, staged in shared memory ...
   while (m) {
@@ -694,14 +700,15 @@ hpt_status hpt_compact(const uint32_t* flags, int32_t n, int32_t* out, int32_t* 
   if (hpt_device_count() == 0) return fail(HPT_ERR_CUDA, "no CUDA device");
   return guarded([&]() -> hpt_status {
     const int nb = blocks_for(n, kCompactTile);
-    DBuf f, o, bc, tot;
+    DBuf f, o, bc, tot, mk;
     hpt_status s;
     if ((s = f.up(flags, (size_t)n * 4)) || (s = o.alloc((size_t)n * 4)) ||
-        (s = bc.alloc((size_t)nb * 4)) || (s = tot.alloc(4)))
+        (s = bc.alloc((size_t)nb * 4)) || (s = tot.alloc(4)) ||
+        (s = mk.alloc((size_t)nb * kCompactThreads)))
       return s;
-    k_compact_count<<<nb, kCompactThreads>>>(f.as<uint32_t>(), n, bc.as<int>());
+    k_compact_count<<<nb, kCompactThreads>>>(f.as<uint32_t>(), n, bc.as<int>(), mk.as<uint8_t>());
     k_compact_scan<<<1, 1024>>>(bc.as<int>(), nb, tot.as<int>());
-    k_compact_scatter<<<nb, kCompactThreads>>>(f.as<uint32_t>(), n, bc.as<int>(), o.as<int>());
+    k_compact_scatter<<<nb, kCompactThreads>>>(mk.as<uint8_t>(), bc.as<int>(), o.as<int>());
     HPT_CUDA(cudaGetLastError());
     int total = 0;
     if ((s = tot.down(&total))) return s;
@@ -805,33 +812,43 @@ void hpt_batch_destroy(hpt_batch* batch) { delete batch; }
 
 // ---------------------------------------------------------------------------
 // hpt_compact_noalloc: the compaction kernels over caller-owned device
-// buffers, with the per-block counts in a static device array instead of a
-// cudaMalloc'd one. For callers that cannot allocate device memory where
+// buffers, with the per-block counts and the mask bytes in static device
+// arrays instead of cudaMalloc'd ones. For callers that cannot allocate device memory where
 // they call it (allocation synchronises the device and would stall their
 // stream; a fixed memory budget leaves nothing to allocate).
 // ---------------------------------------------------------------------------
 namespace {
 
-// One count per 2048-flag tile, plus one spare entry: 64 KB per device.
+// One count per 2048-flag tile, plus one spare entry (64 KB per device),
+// and one mask byte per 8 flags (4 MiB per device).
 constexpr int kNoallocMaxBlocks = HPT_COMPACT_NOALLOC_MAX_N / kCompactTile;
 static_assert(kNoallocMaxBlocks * kCompactTile == HPT_COMPACT_NOALLOC_MAX_N,
               "the limit is a whole number of tiles");
 static __device__ __align__(256) int g_noalloc_block_counts[kNoallocMaxBlocks + 1];
+static __device__ __align__(256) uint8_t g_noalloc_masks[kNoallocMaxBlocks * kCompactThreads];
 
-// Device address of g_noalloc_block_counts, looked up once per device with
-// that device current (the first call on a device does this set-up). The
-// cached address belongs to the device's current context: after a
+struct NoallocScratch {
+  int* counts = nullptr;
+  uint8_t* masks = nullptr;
+};
+
+// Device addresses of the static scratch arrays, looked up once per device
+// with that device current (the first call on a device does this set-up).
+// The cached addresses belong to the device's current context: after a
 // cudaDeviceReset the caller must not use this entry point again in the
 // same process.
-hpt_status noalloc_scratch(int device, int** out) {
+hpt_status noalloc_scratch(int device, NoallocScratch* out) {
   static std::mutex mu;
-  static std::vector<int*> addr;
+  static std::vector<NoallocScratch> addr;
   std::lock_guard<std::mutex> lk(mu);
-  if ((int)addr.size() <= device) addr.resize(device + 1, nullptr);
-  if (!addr[device]) {
-    void* p = nullptr;
-    HPT_CUDA(cudaGetSymbolAddress(&p, g_noalloc_block_counts));
-    addr[device] = static_cast<int*>(p);
+  if ((int)addr.size() <= device) addr.resize(device + 1);
+  if (!addr[device].counts) {
+    void* c = nullptr;
+    void* m = nullptr;
+    HPT_CUDA(cudaGetSymbolAddress(&c, g_noalloc_block_counts));
+    HPT_CUDA(cudaGetSymbolAddress(&m, g_noalloc_masks));
+    addr[device].counts = static_cast<int*>(c);
+    addr[device].masks = static_cast<uint8_t*>(m);
   }
   *out = addr[device];
   return HPT_OK;
@@ -849,7 +866,7 @@ extern "C" hpt_status hpt_compact_noalloc(const uint32_t* flags, int32_t n, int3
                 HPT_COMPACT_NOALLOC_MAX_N);
   int device = 0;
   HPT_CUDA(cudaGetDevice(&device));
-  int* scratch = nullptr;
+  NoallocScratch scratch;
   // The lookup table may grow (host memory): no exception leaves the ABI.
   hpt_status s = guarded([&]() -> hpt_status { return noalloc_scratch(device, &scratch); });
   if (s != HPT_OK) return s;
@@ -861,9 +878,9 @@ extern "C" hpt_status hpt_compact_noalloc(const uint32_t* flags, int32_t n, int3
   const int nb = blocks_for(n, kCompactTile);
   // Every entry [0, nb) is written by the count pass before the scan reads
   // it; the total goes straight to the caller's counter.
-  k_compact_count<<<nb, kCompactThreads, 0, st>>>(flags, n, scratch);
-  k_compact_scan<<<1, 1024, 0, st>>>(scratch, nb, count);
-  k_compact_scatter<<<nb, kCompactThreads, 0, st>>>(flags, n, scratch, out);
+  k_compact_count<<<nb, kCompactThreads, 0, st>>>(flags, n, scratch.counts, scratch.masks);
+  k_compact_scan<<<1, 1024, 0, st>>>(scratch.counts, nb, count);
+  k_compact_scatter<<<nb, kCompactThreads, 0, st>>>(scratch.masks, scratch.counts, out);
   HPT_CUDA(cudaGetLastError());
   return HPT_OK;
 }

@@ -54,6 +54,12 @@ struct EngineParams {
   int32_t* quota_prefix;
   const int32_t* prim_slot;
   const int64_t* prim_prefix;
+  // Primary passes over part of a job's rays (null: every entry covers its
+  // job from ray 0 and completes its primary pass): entry e covers rays
+  // [prim_first[e], prim_first[e] + its count); prim_final[e] != 0 marks
+  // the part that completes the job's primary pass.
+  const int64_t* prim_first;
+  const int32_t* prim_final;
   int prim_n;
   float4* A_o[2];
   float4* A_d[2];
@@ -281,7 +287,7 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
         if (g < total) {
           const int e = find_prefix(P.prim_prefix, P.prim_n, g);
           slot = P.prim_slot[e];
-          ray = g - P.prim_prefix[e];
+          ray = g - P.prim_prefix[e] + (P.prim_first ? P.prim_first[e] : 0);
           bool ok = true;
           HPT_DCHECK(&c->err, slot >= 0 && slot < P.num_slots, 201, slot, ok = false);
           HPT_DCHECK(&c->err, !ok || (ray >= 0 && ray < job_rays(P.jobs[slot])), 202, ray,
@@ -353,7 +359,9 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
   flush_counts(c, queries, cnt);
 }
 
-// Sets the path counts of newly admitted slots and grants paths (one thread).
+// Sets the path counts of the slots whose primary pass completed and grants
+// paths (one thread). A slot whose primary pass is still partial stays as
+// it was: inactive, or finished with nothing left to issue.
 __global__ void k_admit(EngineParams P) {
 #ifdef HPT_DEVICE_CHECKS
   HPT_DCHECK(&P.ctrl->err, P.ctrl->chk_isect_done == P.prim_prefix[P.prim_n], 243,
@@ -363,6 +371,7 @@ __global__ void k_admit(EngineParams P) {
   for (int e = 0; e < P.prim_n; ++e) {
     const int s = P.prim_slot[e];
     HPT_DCHECK(&P.ctrl->err, s >= 0 && s < P.num_slots, 232, s, continue);
+    if (P.prim_final && !P.prim_final[e]) continue;
     DevSlot& S = P.slots[s];
     S.num_paths = (int64_t)(*P.jobs[s].prim_count) * P.jobs[s].spp;
     S.cursor = 0;
@@ -903,6 +912,8 @@ Engine::~Engine() {
   HPT_SOFT(cudaFree(quota_prefix_));
   HPT_SOFT(cudaFree(prim_slot_));
   HPT_SOFT(cudaFree(prim_prefix_));
+  HPT_SOFT(cudaFree(prim_first_));
+  HPT_SOFT(cudaFree(prim_final_));
   HPT_SOFT(cudaFreeHost(ctrl_host_));
   HPT_SOFT(cudaFreeHost(host_i32_));
   HPT_SOFT(cudaFreeHost(host_i64_));
@@ -971,6 +982,8 @@ hpt_status Engine::ensure_slots(int slots) {
   HPT_SOFT(cudaFree(quota_prefix_));
   HPT_SOFT(cudaFree(prim_slot_));
   HPT_SOFT(cudaFree(prim_prefix_));
+  HPT_SOFT(cudaFree(prim_first_));
+  HPT_SOFT(cudaFree(prim_final_));
   HPT_SOFT(cudaFreeHost(host_i32_));
   HPT_SOFT(cudaFreeHost(host_i64_));
   HPT_SOFT(cudaFreeHost(host_jobs_));
@@ -978,8 +991,8 @@ hpt_status Engine::ensure_slots(int slots) {
   slots_host_ = nullptr;
   jobs_ = nullptr;
   slot_state_ = nullptr;
-  order_ = quota_slot_ = quota_prefix_ = prim_slot_ = nullptr;
-  prim_prefix_ = nullptr;
+  order_ = quota_slot_ = quota_prefix_ = prim_slot_ = prim_final_ = nullptr;
+  prim_prefix_ = prim_first_ = nullptr;
   host_i32_ = nullptr;
   host_i64_ = nullptr;
   host_jobs_ = nullptr;
@@ -992,6 +1005,8 @@ hpt_status Engine::ensure_slots(int slots) {
   HPT_CUDA(cudaMalloc(&quota_prefix_, (n + 1) * sizeof(int32_t)));
   HPT_CUDA(cudaMalloc(&prim_slot_, n * sizeof(int32_t)));
   HPT_CUDA(cudaMalloc(&prim_prefix_, (n + 1) * sizeof(int64_t)));
+  HPT_CUDA(cudaMalloc(&prim_first_, n * sizeof(int64_t)));
+  HPT_CUDA(cudaMalloc(&prim_final_, n * sizeof(int32_t)));
   HPT_CUDA(cudaMallocHost(&host_i32_, (2 * n + 3) * sizeof(int32_t)));
   HPT_CUDA(cudaMallocHost(&host_i64_, (n + 1) * sizeof(int64_t)));
   HPT_CUDA(cudaMallocHost(&host_jobs_, n * sizeof(DevJob)));
@@ -1254,8 +1269,8 @@ hpt_status Engine::next_staging(StagingSet** out) {
     const size_t n = (size_t)slots_;
     for (StagingSet& st : staging_) {
       HPT_CUDA(cudaMallocHost(&st.jobs, n * sizeof(DevJob)));
-      HPT_CUDA(cudaMallocHost(&st.i32, (2 * n + 3) * sizeof(int32_t)));
-      HPT_CUDA(cudaMallocHost(&st.i64, (n + 1) * sizeof(int64_t)));
+      HPT_CUDA(cudaMallocHost(&st.i32, (3 * n + 3) * sizeof(int32_t)));
+      HPT_CUDA(cudaMallocHost(&st.i64, (2 * n + 1) * sizeof(int64_t)));
       if (!st.ev) HPT_CUDA(cudaEventCreateWithFlags(&st.ev, cudaEventDisableTiming));
     }
     staging_slots_ = slots_;
@@ -1294,7 +1309,8 @@ hpt_status Engine::set_order_async(const std::vector<int>& order) {
 
 hpt_status Engine::admit_async(const std::vector<int>& slot_ids, const std::vector<DevJob>& jobs,
                                const std::vector<int64_t>& rays, const std::vector<int>& order,
-                               const DevScene* shared_scene) {
+                               const DevScene* shared_scene, const std::vector<int64_t>& first,
+                               const std::vector<int>& final_part) {
   const int n = (int)slot_ids.size();
   if (n == 0) return set_order_async(order);
   hpt_status s = query_occupancy();
@@ -1309,15 +1325,34 @@ hpt_status Engine::admit_async(const std::vector<int>& slot_ids, const std::vect
     HPT_CUDA(cudaMemcpyAsync(jobs_ + slot_ids[k], st->jobs + k, sizeof(DevJob),
                              cudaMemcpyHostToDevice, stream));
   }
+  const bool parts = !first.empty();
+  if (parts && ((int)first.size() != n || (int)final_part.size() != n))
+    return fail(HPT_ERR_INVALID_ARGUMENT, "primary parts: %d entries, %d firsts, %d flags", n,
+                (int)first.size(), (int)final_part.size());
   st->i64[0] = 0;
+  // Staging layout: i32 [0, n) slots, [slots + 1, 2 slots + 2] order (see
+  // upload_order), [2 slots + 3, + n) final flags; i64 [0, n] prefix,
+  // [slots + 1, + n) first rays.
+  int32_t* fin = st->i32 + 2 * slots_ + 3;
+  int64_t* fst = st->i64 + slots_ + 1;
   for (int k = 0; k < n; ++k) {
     st->i32[k] = slot_ids[k];
     st->i64[k + 1] = st->i64[k] + rays[k];
+    if (parts) {
+      fst[k] = first[k];
+      fin[k] = final_part[k];
+    }
   }
   HPT_CUDA(cudaMemcpyAsync(prim_slot_, st->i32, n * sizeof(int32_t), cudaMemcpyHostToDevice,
                            stream));
   HPT_CUDA(cudaMemcpyAsync(prim_prefix_, st->i64, (n + 1) * sizeof(int64_t),
                            cudaMemcpyHostToDevice, stream));
+  if (parts) {
+    HPT_CUDA(cudaMemcpyAsync(prim_first_, fst, n * sizeof(int64_t), cudaMemcpyHostToDevice,
+                             stream));
+    HPT_CUDA(cudaMemcpyAsync(prim_final_, fin, n * sizeof(int32_t), cudaMemcpyHostToDevice,
+                             stream));
+  }
   s = upload_order(order, *st);
   if (s != HPT_OK) return s;
   HPT_CUDA(cudaEventRecord(st->ev, stream));
@@ -1326,6 +1361,10 @@ hpt_status Engine::admit_async(const std::vector<int>& slot_ids, const std::vect
   EngineParams P = make_params(*this, ctrl_, jobs_, slot_state_, slots_, order_, quota_slot_,
                                quota_prefix_, prim_slot_, prim_prefix_, n, capacity_, A, A_tri_,
                                A_leaf_, R, shared_scene);
+  if (parts) {
+    P.prim_first = prim_first_;
+    P.prim_final = prim_final_;
+  }
   const size_t smem = launch_smem(P);
   const IsectVariant& v = kIsectVariants[isect_variant()];
   v.primary_kernel(P.trav_steps, P.smem_nodes)<<<num_sms * occ_isect_, v.block, smem, stream>>>(P);

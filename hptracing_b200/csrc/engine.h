@@ -80,9 +80,16 @@ class Engine {
   // Asynchronous forms for a serving loop: the uploads go through a ring of
   // pinned staging sets and nothing waits for the stream (only, rarely, for
   // a staging set's previous copies to have run).
+  // With `first` and `final_part` (one entry per slot), entry k traces rays
+  // [first[k], first[k] + rays[k]) of its job, and only an entry with
+  // final_part[k] != 0 starts the job's paths: a large job's primary pass
+  // can be split over several calls (same slot, same job, consecutive
+  // ranges, the last one final) so that no single launch stalls the
+  // iterations of the others for long.
   hpt_status admit_async(const std::vector<int>& slot_ids, const std::vector<DevJob>& jobs,
                          const std::vector<int64_t>& rays, const std::vector<int>& order,
-                         const DevScene* shared_scene);
+                         const DevScene* shared_scene, const std::vector<int64_t>& first = {},
+                         const std::vector<int>& final_part = {});
   hpt_status set_order_async(const std::vector<int>& order);
   // Enqueues a copy of the slot table and control block into pinned host
   // memory and records ev after it.
@@ -120,6 +127,8 @@ class Engine {
   int32_t* quota_prefix_ = nullptr;
   int32_t* prim_slot_ = nullptr;
   int64_t* prim_prefix_ = nullptr;
+  int64_t* prim_first_ = nullptr;
+  int32_t* prim_final_ = nullptr;
   int32_t* host_i32_ = nullptr;   // pinned staging for small uploads
   int64_t* host_i64_ = nullptr;
   DevJob* host_jobs_ = nullptr;

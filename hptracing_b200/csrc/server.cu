@@ -24,6 +24,7 @@
 #include <cstring>
 #include <deque>
 #include <fstream>
+#include <limits>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -68,7 +69,9 @@ struct Request {
   bool cancel = false;
   bool finishing = false;   // resolve and copy-back enqueued
   cudaEvent_t fin_ev = nullptr;
-  uint64_t admit_seq = 0;   // iterations launched before its admission
+  uint64_t admit_seq = 0;   // iterations launched before its primary pass completed
+  int64_t prim_next = 0;    // rays whose primary pass has been enqueued
+  DevJob dj{};              // the job as admitted (for the later parts of its primary pass)
   JobBuffers buf;
   int64_t footprint = 0;
   int64_t rays = 0;
@@ -133,6 +136,10 @@ struct hpt_server {
   double last_small_done_ms = 0;
   double tail_ms = 0;  // predicted completion of the latest admitted latency-bound request
   double drift_ms = 0;  // sum of the corrections applied to the predictions so far
+  // Fraction of the deadline that admissions aim at: cut by 15 % whenever a
+  // served latency-bound request finishes late, raised by 0.001 when one
+  // finishes in time, so that about one in a hundred finishes late.
+  double slack = 1.0;
   int64_t shed = 0;
 
   double now_ms() const {
@@ -212,8 +219,43 @@ struct hpt_server {
 hpt_status hpt_server::admit_pending() {
   std::vector<int> ids;
   std::vector<DevJob> jobs;
-  std::vector<int64_t> rays;
+  std::vector<int64_t> rays, first;
+  std::vector<int> final_part;
   const double now = now_ms();
+  // Primary passes are split into parts of at most a quarter of the
+  // wavefront, and at most that many rays of large requests are traced per
+  // pump, so that a large request's primary pass never stalls the
+  // iterations of the requests in flight for long. A request whose rays fit
+  // in one part (every latency-bound one at the default sizes) is traced
+  // whole at admission.
+  const int64_t part = std::max<int64_t>(1024, cfg.capacity / 4);
+  int64_t large_budget = part;
+  auto enqueue_part = [&](Request* r) {
+    const int64_t n = std::min(part, r->rays - r->prim_next);
+    ids.push_back(r->slot);
+    jobs.push_back(r->dj);
+    rays.push_back(n);
+    first.push_back(r->prim_next);
+    r->prim_next += n;
+    const bool last = r->prim_next == r->rays;
+    final_part.push_back(last ? 1 : 0);
+    // Read-backs count the request only once its paths exist.
+    r->admit_seq = last ? launched : std::numeric_limits<uint64_t>::max();
+    if (!r->small) large_budget -= n;
+  };
+  {
+    // Requests part-way through their primary pass, oldest first.
+    std::vector<Request*> priming;
+    for (size_t k = 0; k < slot_req.size(); ++k)
+      if (slot_req[k]) {
+        Request* r = reqs.at(slot_req[k]).get();
+        if (r->prim_next < r->rays) priming.push_back(r);
+      }
+    std::sort(priming.begin(), priming.end(),
+              [](const Request* a, const Request* b) { return a->id < b->id; });
+    for (Request* r : priming)
+      if (r->small || large_budget > 0) enqueue_part(r);
+  }
   bool busy = cfg.deadline_ms > 0 && small_running();
   for (auto it = queue.begin(); it != queue.end();) {
     Request* r = find(*it);
@@ -233,8 +275,9 @@ hpt_status hpt_server::admit_pending() {
       // wait (without holding back younger requests that fit) until they
       // fit or are shed.
       const double waited = now - r->submit_ms;
+      const double target = slack * cfg.deadline_ms;
       ServiceEstimate& e = estimate(r->scene_slot);
-      if (waited > cfg.deadline_ms || (e.alone >= 0 && waited + e.alone > cfg.deadline_ms)) {
+      if (waited > cfg.deadline_ms || (e.alone >= 0 && waited + e.alone > target)) {
         // A stale estimate would shed this scene's requests for good:
         // every shed lowers it a little so that one is measured again.
         if (e.alone >= 0) e.alone *= 0.98;
@@ -248,7 +291,7 @@ hpt_status hpt_server::admit_pending() {
       if (e.alone >= 0) {
         due = now + e.alone;
         if (busy) due = std::max(due, tail_ms + (e.gap >= 0 ? e.gap : e.alone));
-        if (due - r->submit_ms > cfg.deadline_ms) {
+        if (due - r->submit_ms > target) {
           ++it;
           continue;
         }
@@ -256,6 +299,10 @@ hpt_status hpt_server::admit_pending() {
         ++it;  // one request measures a new scene before more are admitted
         continue;
       }
+    }
+    if (!r->small && large_budget <= 0) {
+      ++it;  // this pump's primary rays of large requests are spent
+      continue;
     }
     int slot = -1;
     for (size_t k = 0; k < slot_req.size(); ++k)
@@ -279,7 +326,6 @@ hpt_status hpt_server::admit_pending() {
     r->slot = slot;
     r->state = kRunning;
     r->admit_ms = now_ms();
-    r->admit_seq = launched;
     if (cfg.deadline_ms > 0 && r->small) {
       r->due_ms = due;
       r->drift_ms = drift_ms;
@@ -290,18 +336,17 @@ hpt_status hpt_server::admit_pending() {
     }
     slot_req[slot] = r->id;
     used_bytes += r->footprint;
-    ids.push_back(slot);
-    DevJob dj = engine->make_job(r->js, r->buf);
+    r->dj = engine->make_job(r->js, r->buf);
     const int pct = cfg.large_inflight_pct;
     if (pct > 0 && pct < 100 && r->rays * r->js.params.sample > (int64_t)cfg.capacity)
-      dj.max_inflight = std::max<int64_t>(1024, (int64_t)cfg.capacity * pct / 100);
-    jobs.push_back(dj);
-    rays.push_back(r->rays);
+      r->dj.max_inflight = std::max<int64_t>(1024, (int64_t)cfg.capacity * pct / 100);
+    r->prim_next = 0;
+    enqueue_part(r);
     it = queue.erase(it);
   }
   if (ids.empty()) return HPT_OK;
   HPT_TRACE_BEGIN(admit_async);
-  const hpt_status s = engine->admit_async(ids, jobs, rays, order(), nullptr);
+  const hpt_status s = engine->admit_async(ids, jobs, rays, order(), nullptr, first, final_part);
   HPT_TRACE_END(admit_async);
   return s;
 }
@@ -393,6 +438,10 @@ hpt_status hpt_server::retire_finished() {
       else
         track(e.gap, r->done_ms - std::max(r->admit_ms, last_small_done_ms));
       last_small_done_ms = r->done_ms;
+      if (r->done_ms - r->submit_ms > cfg.deadline_ms)
+        slack = std::max(0.25, slack * 0.85);
+      else
+        slack = std::min(1.0, slack + 0.001);
       // Requests admitted behind this one finish as much earlier or later
       // than predicted as it did (its prediction already moved by the
       // corrections made since its admission).

@@ -204,6 +204,37 @@ def test_autotune_picks_a_valid_tuning_and_caches_it(scenes):
     assert np.array_equal(got, want)
 
 
+def test_primary_pass_in_parts_keeps_results(scenes):
+    """A request with more rays than a quarter of the wavefront has its
+    primary pass traced in parts over several pumps (at most a quarter of
+    the wavefront of large requests' rays per pump), while smaller requests
+    admitted meanwhile run. Capacity 2^12 makes parts of 1,024 rays: the
+    128x96 panorama is twelve parts, the 80x64 request five and the 4x4
+    supersampled 24x16 one six; all must equal the same requests rendered
+    alone."""
+    reqs = [
+        (0, S.PANO_CAM, 128, 96, 1, 3, 6, (0.2, 0.3, 0.4), 401),
+        (1, S.ROOM_CAM, 32, 32, 1, 2, 5, (0, 0, 0), 402),
+        (1, S.ROOM_CAM, 80, 64, 1, 1, 6, (0.1, 0.1, 0.1), 403),
+        (0, S.ROOM_CAM, 24, 16, 4, 2, 6, (0, 0, 0), 404),
+        (0, S.ROOM_CAM, 16, 16, 1, 4, 6, (0, 0, 0), 405),
+    ]
+    server = H.Server(max_jobs=8, memory_budget=1 << 30, capacity=1 << 12, large_inflight_pct=25)
+    slots = [server.add_scene(s) for s in scenes]
+    ids = [server.submit(slots[r[0]], S.hp_camera(r[1]), _params(r)) for r in reqs[:3]]
+    server.pump(1)
+    ids += [server.submit(slots[r[0]], S.hp_camera(r[1]), _params(r)) for r in reqs[3:]]
+    out = _drain(server, ids, reqs)
+    for rid, req in zip(ids, reqs):
+        rgba, acc, info = out[rid]
+        a_rgba, a_acc = _alone(scenes, req)
+        assert np.array_equal(acc, a_acc), req
+        assert np.array_equal(rgba, a_rgba), req
+        assert info["intersect_queries"] > 0
+    assert server.stats()["error_flags"] == 0
+    server.close()
+
+
 def test_overload_policy_sheds_late_requests_and_keeps_results(scenes):
     """deadline_ms: latency-bound requests (<= capacity paths) are admitted
     when predicted to finish in time and shed once they cannot. A burst of
