@@ -647,6 +647,7 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, duration, capacity, la
     lat = {"pose": [], "pano": []}
     shed = {"pose": 0, "pano": 0}
     per_scene = {}
+    sub_at, served_poses = {}, []
     pumps, gaps, last_pump_end = [], [], None
     samples = 0
     nxt = 0
@@ -657,6 +658,7 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, duration, capacity, la
             _, kind, k, cam, p = arrivals[nxt]
             rid = server.submit(slots[k], S.hp_camera(cam), p)
             outstanding[rid] = (kind, p, k)
+            sub_at[rid] = now * 1e3
             nxt += 1
         if not outstanding and nxt >= len(arrivals):
             break
@@ -684,6 +686,13 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, duration, capacity, la
                         (info["done_ms"] - info["submit_ms"], info["admit_ms"] - info["submit_ms"],
                          info["submit_ms"]))
                     samples += p.sample_x * p.sample_y * p.sample
+                    if kind == "pose":
+                        served_poses.append({
+                            "scene": k, "submitted_at_ms": sub_at.get(rid),
+                            "admit_wait_ms": info["admit_ms"] - info["submit_ms"],
+                            "latency_ms": info["done_ms"] - info["submit_ms"],
+                            "done_minus_predicted_ms": (info["done_ms"] - info["due_ms"]
+                                                        if info["due_ms"] >= 0 else None)})
         else:
             time.sleep(0.0005)
     elapsed = time.perf_counter() - start
@@ -724,6 +733,7 @@ def serve_stream(H, S, scenes, cams, tris, build_s, rate, duration, capacity, la
             "n": len(v), "p50_ms": pct([x[0] for x in v], 50), "p99_ms": pct([x[0] for x in v], 99),
             "max_ms": max(x[0] for x in v), "admit_wait_max_ms": max(x[1] for x in v),
             "slowest_submitted_at_ms": max(v)[2]} for key, v in sorted(per_scene.items())},
+        "slowest_poses": sorted(served_poses, key=lambda x: -x["latency_ms"])[:6],
         "host_loop": {"pumps": len(pumps),
                       "pump_ms_p50": pct([x[1] for x in pumps], 50),
                       "slowest_pumps_at_ms": sorted(pumps, key=lambda x: -x[1])[:5],

@@ -105,7 +105,7 @@ class ServerConfig(C.Structure):
 
 class RequestInfo(C.Structure):
     _fields_ = [("state", i32), ("samples_done", i32), ("submit_ms", f64), ("admit_ms", f64),
-                ("done_ms", f64), ("intersect_queries", i64)]
+                ("done_ms", f64), ("intersect_queries", i64), ("due_ms", f64)]
 
 
 # name -> (restype, argtypes); every function declared in include/hpt.h.

@@ -160,18 +160,28 @@ __global__ void k_stage_resolve(const float* accum, int W, int H, int ssx, int s
   out[3] = 0;
 }
 
-// --- Stream compaction: per-tile counts, one scan, stable scatter. -------
+// --- Stream compaction: per-tile counts, then a stable scatter. ----------
 // A tile is 2048 flags: 256 threads x 8 consecutive flags, read as two
 // 16-byte loads where the flag array is 16-byte aligned and the tile is
 // whole. The flags are read once: the count pass also stores each thread's
 // 8 flags as one mask byte (n / 8 bytes in all), which the scatter pass
-// reads instead of the flags. No kernel waits on another block: the three
-// passes are ordered by the stream alone.
+// reads instead of the flags. Tiles are grouped into superblocks of
+// 2^shift tiles with shift = ceil(log2(tiles) / 2); the count pass adds
+// each tile's count to its superblock's total, and the scatter pass finds a
+// tile's output offset by summing at most 2^shift superblock totals and
+// 2^shift tile counts (L2-resident) instead of waiting for a scan. No
+// kernel waits on another block: the two passes are ordered by the stream.
 constexpr int kCompactThreads = 256;
 constexpr int kCompactItems = 8;
 constexpr int kCompactTile = kCompactThreads * kCompactItems;
-constexpr int kScanThreads = 1024;
-constexpr int kScanItems = 16;
+constexpr int kCompactBlocksPerSm = 8;  // 8.3 KB of shared memory per scatter block
+
+inline int compact_super_shift(int tiles) {
+  int s = 0;
+  while ((int64_t)1 << (2 * s) < tiles) ++s;
+  return s;
+}
+inline int compact_supers(int tiles, int shift) { return (tiles + (1 << shift) - 1) >> shift; }
 
 // This thread's 8 flags as a bit mask (bit k: flag i0 + k nonzero).
 __device__ __forceinline__ uint32_t load_flags8(const uint32_t* flags, int64_t i0, int n,
@@ -217,78 +227,84 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
   return warp_tot[warp] + inc - v;
 }
 
-__global__ void __launch_bounds__(kCompactThreads) k_compact_count(const uint32_t* flags, int n,
-                                                                   int* block_counts,
-                                                                   uint8_t* masks) {
+__global__ void __launch_bounds__(kCompactThreads)
+    k_compact_count(const uint32_t* flags, int n, int shift, int* tile_counts, int* super_counts,
+                    uint8_t* masks) {
   __shared__ int warp_sum[kCompactThreads / 32];
   const bool vec = (reinterpret_cast<uintptr_t>(flags) & 15) == 0;
   const int64_t i0 = (int64_t)blockIdx.x * kCompactTile + (int64_t)threadIdx.x * kCompactItems;
   const uint32_t m = load_flags8(flags, i0, n, vec);
   masks[(int64_t)blockIdx.x * kCompactThreads + threadIdx.x] = (uint8_t)m;
-  const int c = __popc(m);
-  const int w = __reduce_add_sync(0xFFFFFFFFu, c);
+  const int w = __reduce_add_sync(0xFFFFFFFFu, __popc(m));
   if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = w;
   __syncthreads();
   if (threadIdx.x == 0) {
     int sum = 0;
     for (int k = 0; k < kCompactThreads / 32; ++k) sum += warp_sum[k];
-    block_counts[blockIdx.x] = sum;
+    tile_counts[blockIdx.x] = sum;
+    if (sum) atomicAdd(&super_counts[blockIdx.x >> shift], sum);
   }
 }
 
-// Exclusive scan of the tile counts in place (one block; 16 consecutive
-// counts per thread per chunk of 16,384), total to *total.
-__global__ void __launch_bounds__(kScanThreads) k_compact_scan(int* counts, int nb, int* total) {
-  __shared__ int chunk_total;
-  int carry = 0;
-  for (int base = 0; base < nb; base += kScanThreads * kScanItems) {
-    const int j0 = base + threadIdx.x * kScanItems;
-    int v[kScanItems];
-    int sum = 0;
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-      v[k] = j0 + k < nb ? counts[j0 + k] : 0;
-      sum += v[k];
-    }
-    int tot = 0;
-    int off = block_exclusive_scan<kScanThreads>(sum, &chunk_total);
-    tot = chunk_total;
-    off += carry;
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-      if (j0 + k < nb) counts[j0 + k] = off;
-      off += v[k];
-    }
-    carry += tot;
-    __syncthreads();  // chunk_total is rewritten by the next chunk
-  }
-  if (threadIdx.x == 0) *total = carry;
-}
-
-// Mask bytes of flags at or past n are zero (the count pass bounds-checks),
-// so the scatter needs no n.
-__global__ void __launch_bounds__(kCompactThreads) k_compact_scatter(const uint8_t* masks,
-                                                                     const int* block_offsets,
-                                                                     int* out) {
+// Blocks stride over the tiles. Mask bytes of flags at or past n are zero
+// (the count pass bounds-checks), so the scatter needs no n. The block that
+// scatters the last tile writes the survivor total.
+__global__ void __launch_bounds__(kCompactThreads)
+    k_compact_scatter(const uint8_t* masks, int tiles, int shift, const int* tile_counts,
+                      const int* super_counts, int* out, int* total) {
   __shared__ int staged[kCompactTile];
   __shared__ int tile_count;
-  const int64_t tile = (int64_t)blockIdx.x * kCompactTile;
-  const int64_t i0 = tile + (int64_t)threadIdx.x * kCompactItems;
-  uint32_t m = masks[(int64_t)blockIdx.x * kCompactThreads + threadIdx.x];
-  int pos = block_exclusive_scan<kCompactThreads>(__popc(m), &tile_count);
-  // Survivor indices of the tile in order, staged in shared memory ...
-  while (m) {
-    const int k = __ffs(m) - 1;
-    m &= m - 1;
-    staged[pos++] = (int)(i0 + k);
+  __shared__ int before[kCompactThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int b = blockIdx.x; b < tiles; b += gridDim.x) {
+    // Survivors of the earlier superblocks, then of this superblock's
+    // earlier tiles.
+    const int sb = b >> shift;
+    int acc = 0;
+    for (int i = threadIdx.x; i < sb; i += kCompactThreads) acc += super_counts[i];
+    for (int i = (sb << shift) + threadIdx.x; i < b; i += kCompactThreads) acc += tile_counts[i];
+    acc = __reduce_add_sync(0xFFFFFFFFu, acc);
+    if (lane == 0) before[warp] = acc;
+    const int64_t i0 = (int64_t)b * kCompactTile + (int64_t)threadIdx.x * kCompactItems;
+    uint32_t m = masks[(int64_t)b * kCompactThreads + threadIdx.x];
+    // (The scan's barriers also publish before[] and tile_count.)
+    int pos = block_exclusive_scan<kCompactThreads>(__popc(m), &tile_count);
+    // Survivor indices of the tile in order, staged in shared memory ...
+    while (m) {
+      const int k = __ffs(m) - 1;
+      m &= m - 1;
+      staged[pos++] = (int)(i0 + k);
+    }
+    int base = 0;
+#pragma unroll
+    for (int k = 0; k < kCompactThreads / 32; ++k) base += before[k];
+    __syncthreads();
+    // ... then written out with consecutive threads on consecutive slots.
+    for (int k = threadIdx.x; k < tile_count; k += kCompactThreads) out[base + k] = staged[k];
+    if (b == tiles - 1 && threadIdx.x == 0) *total = base + tile_count;
+    __syncthreads();  // staged, tile_count and before[] are rewritten for the next tile
   }
-  __syncthreads();
-  // ... then written out with consecutive threads on consecutive slots.
-  const int base = block_offsets[blockIdx.x];
-  for (int k = threadIdx.x; k < tile_count; k += kCompactThreads) out[base + k] = staged[k];
 }
 
 inline int blocks_for(int64_t n, int bs) { return (int)((n + bs - 1) / bs); }
+
+// Enqueues the two compaction passes on `st`. Scratch: tile_counts (tiles
+// ints), super_counts (compact_supers(tiles, shift) ints, zeroed here) and
+// masks (tiles * 256 bytes); the survivor count goes to *total.
+cudaError_t launch_compact(const uint32_t* flags, int n, int* tile_counts, int* super_counts,
+                           uint8_t* masks, int* out, int* total, int sms, cudaStream_t st) {
+  const int tiles = blocks_for(n, kCompactTile);
+  const int shift = compact_super_shift(tiles);
+  cudaError_t e = cudaMemsetAsync(super_counts, 0,
+                                  (size_t)compact_supers(tiles, shift) * sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  k_compact_count<<<tiles, kCompactThreads, 0, st>>>(flags, n, shift, tile_counts, super_counts,
+                                                     masks);
+  const int grid = std::min(tiles, std::max(1, sms) * kCompactBlocksPerSm);
+  k_compact_scatter<<<grid, kCompactThreads, 0, st>>>(masks, tiles, shift, tile_counts,
+                                                      super_counts, out, total);
+  return cudaGetLastError();
+}
 
 hpt_status check_scene_desc(const hpt_scene_desc& d) {
   if (d.num_points < 0 || d.num_triangles <= 0 || d.num_nodes <= 0 || d.num_leaf_data < 0 ||
@@ -700,16 +716,18 @@ hpt_status hpt_compact(const uint32_t* flags, int32_t n, int32_t* out, int32_t* 
   if (hpt_device_count() == 0) return fail(HPT_ERR_CUDA, "no CUDA device");
   return guarded([&]() -> hpt_status {
     const int nb = blocks_for(n, kCompactTile);
-    DBuf f, o, bc, tot, mk;
+    const int ns = compact_supers(nb, compact_super_shift(nb));
+    int device = 0, sms = 0;
+    HPT_CUDA(cudaGetDevice(&device));
+    HPT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    DBuf f, o, bc, sc, tot, mk;
     hpt_status s;
     if ((s = f.up(flags, (size_t)n * 4)) || (s = o.alloc((size_t)n * 4)) ||
-        (s = bc.alloc((size_t)nb * 4)) || (s = tot.alloc(4)) ||
-        (s = mk.alloc((size_t)nb * kCompactThreads)))
+        (s = bc.alloc((size_t)nb * 4)) || (s = sc.alloc((size_t)ns * 4)) ||
+        (s = tot.alloc(4)) || (s = mk.alloc((size_t)nb * kCompactThreads)))
       return s;
-    k_compact_count<<<nb, kCompactThreads>>>(f.as<uint32_t>(), n, bc.as<int>(), mk.as<uint8_t>());
-    k_compact_scan<<<1, 1024>>>(bc.as<int>(), nb, tot.as<int>());
-    k_compact_scatter<<<nb, kCompactThreads>>>(mk.as<uint8_t>(), bc.as<int>(), o.as<int>());
-    HPT_CUDA(cudaGetLastError());
+    HPT_CUDA(launch_compact(f.as<uint32_t>(), n, bc.as<int>(), sc.as<int>(), mk.as<uint8_t>(),
+                            o.as<int>(), tot.as<int>(), sms, 0));
     int total = 0;
     if ((s = tot.down(&total))) return s;
     if (total > 0) HPT_CUDA(cudaMemcpy(out, o.p, (size_t)total * 4, cudaMemcpyDeviceToHost));
@@ -819,17 +837,24 @@ void hpt_batch_destroy(hpt_batch* batch) { delete batch; }
 // ---------------------------------------------------------------------------
 namespace {
 
-// One count per 2048-flag tile, plus one spare entry (64 KB per device),
-// and one mask byte per 8 flags (4 MiB per device).
+// One count per 2048-flag tile (64 KB per device), one total per
+// superblock of 128 tiles (16,384 tiles need 128), and one mask byte per 8
+// flags (4 MiB per device).
 constexpr int kNoallocMaxBlocks = HPT_COMPACT_NOALLOC_MAX_N / kCompactTile;
 static_assert(kNoallocMaxBlocks * kCompactTile == HPT_COMPACT_NOALLOC_MAX_N,
               "the limit is a whole number of tiles");
-static __device__ __align__(256) int g_noalloc_block_counts[kNoallocMaxBlocks + 1];
+constexpr int kNoallocMaxSupers = 128;
+static_assert(kNoallocMaxBlocks <= kNoallocMaxSupers * kNoallocMaxSupers,
+              "superblocks of at most 128 tiles cover the limit");
+static __device__ __align__(256) int g_noalloc_block_counts[kNoallocMaxBlocks];
+static __device__ __align__(256) int g_noalloc_super_counts[kNoallocMaxSupers];
 static __device__ __align__(256) uint8_t g_noalloc_masks[kNoallocMaxBlocks * kCompactThreads];
 
 struct NoallocScratch {
   int* counts = nullptr;
+  int* supers = nullptr;
   uint8_t* masks = nullptr;
+  int sms = 0;
 };
 
 // Device addresses of the static scratch arrays, looked up once per device
@@ -844,11 +869,17 @@ hpt_status noalloc_scratch(int device, NoallocScratch* out) {
   if ((int)addr.size() <= device) addr.resize(device + 1);
   if (!addr[device].counts) {
     void* c = nullptr;
+    void* sc = nullptr;
     void* m = nullptr;
+    int sms = 0;
     HPT_CUDA(cudaGetSymbolAddress(&c, g_noalloc_block_counts));
+    HPT_CUDA(cudaGetSymbolAddress(&sc, g_noalloc_super_counts));
     HPT_CUDA(cudaGetSymbolAddress(&m, g_noalloc_masks));
+    HPT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     addr[device].counts = static_cast<int*>(c);
+    addr[device].supers = static_cast<int*>(sc);
     addr[device].masks = static_cast<uint8_t*>(m);
+    addr[device].sms = sms;
   }
   *out = addr[device];
   return HPT_OK;
@@ -875,12 +906,9 @@ extern "C" hpt_status hpt_compact_noalloc(const uint32_t* flags, int32_t n, int3
     HPT_CUDA(cudaMemsetAsync(count, 0, sizeof(int32_t), st));
     return HPT_OK;
   }
-  const int nb = blocks_for(n, kCompactTile);
-  // Every entry [0, nb) is written by the count pass before the scan reads
+  // Every tile count is written by the count pass before the scatter reads
   // it; the total goes straight to the caller's counter.
-  k_compact_count<<<nb, kCompactThreads, 0, st>>>(flags, n, scratch.counts, scratch.masks);
-  k_compact_scan<<<1, 1024, 0, st>>>(scratch.counts, nb, count);
-  k_compact_scatter<<<nb, kCompactThreads, 0, st>>>(scratch.masks, scratch.counts, out);
-  HPT_CUDA(cudaGetLastError());
+  HPT_CUDA(launch_compact(flags, n, scratch.counts, scratch.supers, scratch.masks, out, count,
+                          scratch.sms, st));
   return HPT_OK;
 }

@@ -222,16 +222,18 @@ hpt_status hpt_server::admit_pending() {
   std::vector<int64_t> rays, first;
   std::vector<int> final_part;
   const double now = now_ms();
-  // Primary passes are split into parts of at most a quarter of the
-  // wavefront, and at most that many rays of large requests are traced per
-  // pump, so that a large request's primary pass never stalls the
-  // iterations of the requests in flight for long. A request whose rays fit
-  // in one part (every latency-bound one at the default sizes) is traced
-  // whole at admission.
-  const int64_t part = std::max<int64_t>(1024, cfg.capacity / 4);
-  int64_t large_budget = part;
+  // A latency-bound request's primary pass is traced whole at admission.
+  // A large request's is traced in parts, at most its in-flight share of
+  // the wavefront (large_inflight_pct, else a quarter) of rays per pump for
+  // all large requests together: one panorama's 2M camera rays traced in
+  // one launch would stall every request in flight for milliseconds.
+  const int pct = cfg.large_inflight_pct;
+  const int64_t share = pct > 0 && pct < 100 ? (int64_t)cfg.capacity * pct / 100
+                                             : (int64_t)cfg.capacity / 4;
+  int64_t large_budget = std::max<int64_t>(1024, share);
   auto enqueue_part = [&](Request* r) {
-    const int64_t n = std::min(part, r->rays - r->prim_next);
+    const int64_t left = r->rays - r->prim_next;
+    const int64_t n = r->small ? left : std::min(left, std::max<int64_t>(1024, large_budget));
     ids.push_back(r->slot);
     jobs.push_back(r->dj);
     rays.push_back(n);
@@ -337,7 +339,6 @@ hpt_status hpt_server::admit_pending() {
     slot_req[slot] = r->id;
     used_bytes += r->footprint;
     r->dj = engine->make_job(r->js, r->buf);
-    const int pct = cfg.large_inflight_pct;
     if (pct > 0 && pct < 100 && r->rays * r->js.params.sample > (int64_t)cfg.capacity)
       r->dj.max_inflight = std::max<int64_t>(1024, (int64_t)cfg.capacity * pct / 100);
     r->prim_next = 0;
@@ -630,6 +631,7 @@ hpt_status hpt_server_poll(hpt_server* server, uint64_t request_id, hpt_request_
     info->admit_ms = r->admit_ms;
     info->done_ms = r->done_ms;
     info->intersect_queries = r->queries;
+    info->due_ms = r->due_ms;
   }
   if (r->state == kDone) {
     if (rgba_out) std::memcpy(rgba_out, r->rgba, r->rgba_bytes);

@@ -205,13 +205,14 @@ def test_autotune_picks_a_valid_tuning_and_caches_it(scenes):
 
 
 def test_primary_pass_in_parts_keeps_results(scenes):
-    """A request with more rays than a quarter of the wavefront has its
-    primary pass traced in parts over several pumps (at most a quarter of
-    the wavefront of large requests' rays per pump), while smaller requests
-    admitted meanwhile run. Capacity 2^12 makes parts of 1,024 rays: the
-    128x96 panorama is twelve parts, the 80x64 request five and the 4x4
-    supersampled 24x16 one six; all must equal the same requests rendered
-    alone."""
+    """A large request (more paths than the wavefront) has its primary pass
+    traced in parts over several pumps, at most its in-flight share of the
+    wavefront in rays per pump for all large requests together, while the
+    smaller requests admitted meanwhile run. Capacity 2^12 with a 25 %
+    share makes that 1,024 rays per pump: the 128x96 panorama (3 spp), the
+    80x64 request and the 4x4 supersampled 24x16 one take 23 pumps in all,
+    the two small ones are traced whole. All must equal the same requests
+    rendered alone."""
     reqs = [
         (0, S.PANO_CAM, 128, 96, 1, 3, 6, (0.2, 0.3, 0.4), 401),
         (1, S.ROOM_CAM, 32, 32, 1, 2, 5, (0, 0, 0), 402),
