@@ -161,10 +161,10 @@ __global__ void k_stage_resolve(const float* accum, int W, int H, int ssx, int s
 }
 
 // --- Stream compaction: per-tile counts, then a stable scatter. ----------
-// A tile is 2048 flags: 256 threads x 8 consecutive flags, read as two
+// A tile is 4096 flags: 256 threads x 16 consecutive flags, read as four
 // 16-byte loads where the flag array is 16-byte aligned and the tile is
 // whole. The flags are read once: the count pass also stores each thread's
-// 8 flags as one mask byte (n / 8 bytes in all), which the scatter pass
+// 16 flags as a 16-bit mask (n / 8 bytes in all), which the scatter pass
 // reads instead of the flags. Tiles are grouped into superblocks of
 // 2^shift tiles with shift = ceil(log2(tiles) / 2); the count pass adds
 // each tile's count to its superblock's total, and the scatter pass finds a
@@ -172,9 +172,8 @@ __global__ void k_stage_resolve(const float* accum, int W, int H, int ssx, int s
 // 2^shift tile counts (L2-resident) instead of waiting for a scan. No
 // kernel waits on another block: the two passes are ordered by the stream.
 constexpr int kCompactThreads = 256;
-constexpr int kCompactItems = 8;
+constexpr int kCompactItems = 16;
 constexpr int kCompactTile = kCompactThreads * kCompactItems;
-constexpr int kCompactBlocksPerSm = 8;  // 8.3 KB of shared memory per scatter block
 
 inline int compact_super_shift(int tiles) {
   int s = 0;
@@ -183,15 +182,17 @@ inline int compact_super_shift(int tiles) {
 }
 inline int compact_supers(int tiles, int shift) { return (tiles + (1 << shift) - 1) >> shift; }
 
-// This thread's 8 flags as a bit mask (bit k: flag i0 + k nonzero).
-__device__ __forceinline__ uint32_t load_flags8(const uint32_t* flags, int64_t i0, int n,
-                                                bool vec) {
+// This thread's 16 flags as a bit mask (bit k: flag i0 + k nonzero).
+__device__ __forceinline__ uint32_t load_flags16(const uint32_t* flags, int64_t i0, int n,
+                                                 bool vec) {
   uint32_t m = 0;
   if (vec && i0 + kCompactItems <= n) {
-    const uint4 a = __ldg(reinterpret_cast<const uint4*>(flags + i0));
-    const uint4 b = __ldg(reinterpret_cast<const uint4*>(flags + i0) + 1);
+    const uint4* p = reinterpret_cast<const uint4*>(flags + i0);
+    const uint4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
     m = (a.x != 0) | (a.y != 0) << 1 | (a.z != 0) << 2 | (a.w != 0) << 3 | (b.x != 0) << 4 |
-        (b.y != 0) << 5 | (b.z != 0) << 6 | (b.w != 0) << 7;
+        (b.y != 0) << 5 | (b.z != 0) << 6 | (b.w != 0) << 7 | (c.x != 0) << 8 |
+        (c.y != 0) << 9 | (c.z != 0) << 10 | (c.w != 0) << 11 | (d.x != 0) << 12 |
+        (d.y != 0) << 13 | (d.z != 0) << 14 | (d.w != 0) << 15;
   } else {
     for (int k = 0; k < kCompactItems; ++k)
       if (i0 + k < n && __ldg(flags + i0 + k) != 0) m |= 1u << k;
@@ -229,12 +230,12 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
 
 __global__ void __launch_bounds__(kCompactThreads)
     k_compact_count(const uint32_t* flags, int n, int shift, int* tile_counts, int* super_counts,
-                    uint8_t* masks) {
+                    uint16_t* masks) {
   __shared__ int warp_sum[kCompactThreads / 32];
   const bool vec = (reinterpret_cast<uintptr_t>(flags) & 15) == 0;
   const int64_t i0 = (int64_t)blockIdx.x * kCompactTile + (int64_t)threadIdx.x * kCompactItems;
-  const uint32_t m = load_flags8(flags, i0, n, vec);
-  masks[(int64_t)blockIdx.x * kCompactThreads + threadIdx.x] = (uint8_t)m;
+  const uint32_t m = load_flags16(flags, i0, n, vec);
+  masks[(int64_t)blockIdx.x * kCompactThreads + threadIdx.x] = (uint16_t)m;
   const int w = __reduce_add_sync(0xFFFFFFFFu, __popc(m));
   if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = w;
   __syncthreads();
@@ -246,53 +247,53 @@ __global__ void __launch_bounds__(kCompactThreads)
   }
 }
 
-// Blocks stride over the tiles. Mask bytes of flags at or past n are zero
-// (the count pass bounds-checks), so the scatter needs no n. The block that
-// scatters the last tile writes the survivor total.
+// One tile per block. Mask bits of flags at or past n are zero (the count
+// pass bounds-checks), so the scatter needs no n. The block of the last
+// tile writes the survivor total.
 __global__ void __launch_bounds__(kCompactThreads)
-    k_compact_scatter(const uint8_t* masks, int tiles, int shift, const int* tile_counts,
+    k_compact_scatter(const uint16_t* masks, int tiles, int shift, const int* tile_counts,
                       const int* super_counts, int* out, int* total) {
   __shared__ int staged[kCompactTile];
   __shared__ int tile_count;
   __shared__ int before[kCompactThreads / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int b = blockIdx.x; b < tiles; b += gridDim.x) {
-    // Survivors of the earlier superblocks, then of this superblock's
-    // earlier tiles.
-    const int sb = b >> shift;
-    int acc = 0;
-    for (int i = threadIdx.x; i < sb; i += kCompactThreads) acc += super_counts[i];
-    for (int i = (sb << shift) + threadIdx.x; i < b; i += kCompactThreads) acc += tile_counts[i];
-    acc = __reduce_add_sync(0xFFFFFFFFu, acc);
-    if (lane == 0) before[warp] = acc;
-    const int64_t i0 = (int64_t)b * kCompactTile + (int64_t)threadIdx.x * kCompactItems;
-    uint32_t m = masks[(int64_t)b * kCompactThreads + threadIdx.x];
-    // (The scan's barriers also publish before[] and tile_count.)
-    int pos = block_exclusive_scan<kCompactThreads>(__popc(m), &tile_count);
-    // Survivor indices of the tile in order, staged in shared memory ...
-    while (m) {
-      const int k = __ffs(m) - 1;
-      m &= m - 1;
-      staged[pos++] = (int)(i0 + k);
-    }
-    int base = 0;
+  const int b = blockIdx.x;
+  const uint32_t m = masks[(int64_t)b * kCompactThreads + threadIdx.x];
+  // Survivors of the earlier superblocks, then of this superblock's earlier
+  // tiles.
+  const int sb = b >> shift;
+  int acc = 0;
+  for (int i = threadIdx.x; i < sb; i += kCompactThreads) acc += super_counts[i];
+  for (int i = (sb << shift) + threadIdx.x; i < b; i += kCompactThreads) acc += tile_counts[i];
+  acc = __reduce_add_sync(0xFFFFFFFFu, acc);
+  if (lane == 0) before[warp] = acc;
+  // (The scan's barriers also publish before[] and tile_count.)
+  int pos = block_exclusive_scan<kCompactThreads>(__popc(m), &tile_count);
+  // Survivor indices of the tile in order, staged in shared memory (one
+  // predicated store per flag, no loop over set bits) ...
+  const int i0 = (int)((int64_t)b * kCompactTile) + (int)threadIdx.x * kCompactItems;
 #pragma unroll
-    for (int k = 0; k < kCompactThreads / 32; ++k) base += before[k];
-    __syncthreads();
-    // ... then written out with consecutive threads on consecutive slots.
-    for (int k = threadIdx.x; k < tile_count; k += kCompactThreads) out[base + k] = staged[k];
-    if (b == tiles - 1 && threadIdx.x == 0) *total = base + tile_count;
-    __syncthreads();  // staged, tile_count and before[] are rewritten for the next tile
+  for (int k = 0; k < kCompactItems; ++k) {
+    const int bit = (m >> k) & 1;
+    if (bit) staged[pos] = i0 + k;
+    pos += bit;
   }
+  int base = 0;
+#pragma unroll
+  for (int k = 0; k < kCompactThreads / 32; ++k) base += before[k];
+  __syncthreads();
+  // ... then written out with consecutive threads on consecutive slots.
+  for (int k = threadIdx.x; k < tile_count; k += kCompactThreads) out[base + k] = staged[k];
+  if (b == tiles - 1 && threadIdx.x == 0) *total = base + tile_count;
 }
 
 inline int blocks_for(int64_t n, int bs) { return (int)((n + bs - 1) / bs); }
 
 // Enqueues the two compaction passes on `st`. Scratch: tile_counts (tiles
 // ints), super_counts (compact_supers(tiles, shift) ints, zeroed here) and
-// masks (tiles * 256 bytes); the survivor count goes to *total.
+// masks (tiles * 256 16-bit masks); the survivor count goes to *total.
 cudaError_t launch_compact(const uint32_t* flags, int n, int* tile_counts, int* super_counts,
-                           uint8_t* masks, int* out, int* total, int sms, cudaStream_t st) {
+                           uint16_t* masks, int* out, int* total, cudaStream_t st) {
   const int tiles = blocks_for(n, kCompactTile);
   const int shift = compact_super_shift(tiles);
   cudaError_t e = cudaMemsetAsync(super_counts, 0,
@@ -300,9 +301,8 @@ cudaError_t launch_compact(const uint32_t* flags, int n, int* tile_counts, int* 
   if (e != cudaSuccess) return e;
   k_compact_count<<<tiles, kCompactThreads, 0, st>>>(flags, n, shift, tile_counts, super_counts,
                                                      masks);
-  const int grid = std::min(tiles, std::max(1, sms) * kCompactBlocksPerSm);
-  k_compact_scatter<<<grid, kCompactThreads, 0, st>>>(masks, tiles, shift, tile_counts,
-                                                      super_counts, out, total);
+  k_compact_scatter<<<tiles, kCompactThreads, 0, st>>>(masks, tiles, shift, tile_counts,
+                                                       super_counts, out, total);
   return cudaGetLastError();
 }
 
@@ -717,17 +717,14 @@ hpt_status hpt_compact(const uint32_t* flags, int32_t n, int32_t* out, int32_t* 
   return guarded([&]() -> hpt_status {
     const int nb = blocks_for(n, kCompactTile);
     const int ns = compact_supers(nb, compact_super_shift(nb));
-    int device = 0, sms = 0;
-    HPT_CUDA(cudaGetDevice(&device));
-    HPT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     DBuf f, o, bc, sc, tot, mk;
     hpt_status s;
     if ((s = f.up(flags, (size_t)n * 4)) || (s = o.alloc((size_t)n * 4)) ||
         (s = bc.alloc((size_t)nb * 4)) || (s = sc.alloc((size_t)ns * 4)) ||
-        (s = tot.alloc(4)) || (s = mk.alloc((size_t)nb * kCompactThreads)))
+        (s = tot.alloc(4)) || (s = mk.alloc((size_t)nb * kCompactThreads * 2)))
       return s;
-    HPT_CUDA(launch_compact(f.as<uint32_t>(), n, bc.as<int>(), sc.as<int>(), mk.as<uint8_t>(),
-                            o.as<int>(), tot.as<int>(), sms, 0));
+    HPT_CUDA(launch_compact(f.as<uint32_t>(), n, bc.as<int>(), sc.as<int>(), mk.as<uint16_t>(),
+                            o.as<int>(), tot.as<int>(), 0));
     int total = 0;
     if ((s = tot.down(&total))) return s;
     if (total > 0) HPT_CUDA(cudaMemcpy(out, o.p, (size_t)total * 4, cudaMemcpyDeviceToHost));
@@ -837,9 +834,9 @@ void hpt_batch_destroy(hpt_batch* batch) { delete batch; }
 // ---------------------------------------------------------------------------
 namespace {
 
-// One count per 2048-flag tile (64 KB per device), one total per
-// superblock of 128 tiles (16,384 tiles need 128), and one mask byte per 8
-// flags (4 MiB per device).
+// One count per 4096-flag tile (32 KB per device), one total per
+// superblock of at most 128 tiles (8,192 tiles need 64), and 16-bit masks,
+// one per 16 flags (4 MiB per device).
 constexpr int kNoallocMaxBlocks = HPT_COMPACT_NOALLOC_MAX_N / kCompactTile;
 static_assert(kNoallocMaxBlocks * kCompactTile == HPT_COMPACT_NOALLOC_MAX_N,
               "the limit is a whole number of tiles");
@@ -848,13 +845,12 @@ static_assert(kNoallocMaxBlocks <= kNoallocMaxSupers * kNoallocMaxSupers,
               "superblocks of at most 128 tiles cover the limit");
 static __device__ __align__(256) int g_noalloc_block_counts[kNoallocMaxBlocks];
 static __device__ __align__(256) int g_noalloc_super_counts[kNoallocMaxSupers];
-static __device__ __align__(256) uint8_t g_noalloc_masks[kNoallocMaxBlocks * kCompactThreads];
+static __device__ __align__(256) uint16_t g_noalloc_masks[kNoallocMaxBlocks * kCompactThreads];
 
 struct NoallocScratch {
   int* counts = nullptr;
   int* supers = nullptr;
-  uint8_t* masks = nullptr;
-  int sms = 0;
+  uint16_t* masks = nullptr;
 };
 
 // Device addresses of the static scratch arrays, looked up once per device
@@ -871,15 +867,12 @@ hpt_status noalloc_scratch(int device, NoallocScratch* out) {
     void* c = nullptr;
     void* sc = nullptr;
     void* m = nullptr;
-    int sms = 0;
     HPT_CUDA(cudaGetSymbolAddress(&c, g_noalloc_block_counts));
     HPT_CUDA(cudaGetSymbolAddress(&sc, g_noalloc_super_counts));
     HPT_CUDA(cudaGetSymbolAddress(&m, g_noalloc_masks));
-    HPT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     addr[device].counts = static_cast<int*>(c);
     addr[device].supers = static_cast<int*>(sc);
-    addr[device].masks = static_cast<uint8_t*>(m);
-    addr[device].sms = sms;
+    addr[device].masks = static_cast<uint16_t*>(m);
   }
   *out = addr[device];
   return HPT_OK;
@@ -909,6 +902,6 @@ extern "C" hpt_status hpt_compact_noalloc(const uint32_t* flags, int32_t n, int3
   // Every tile count is written by the count pass before the scatter reads
   // it; the total goes straight to the caller's counter.
   HPT_CUDA(launch_compact(flags, n, scratch.counts, scratch.supers, scratch.masks, out, count,
-                          scratch.sms, st));
+                          st));
   return HPT_OK;
 }

@@ -251,6 +251,80 @@ constexpr int kTravLeaf = 0;      // trav_leaf, one leaf per lane per round
 constexpr int kTravStep = 1;      // trav_step, nodes from global memory
 constexpr int kTravStepSmem = 2;  // trav_step with the shared-memory node prefix
 
+#ifndef HPT_PHASE_VOTE
+#define HPT_PHASE_VOTE 0
+#endif
+#if HPT_PHASE_VOTE
+// Up to `units` warp rounds of the step-at-a-time walk in which only the
+// lanes of the more common phase (descent / leaf set-up, or triangle test)
+// run a unit, so that a round executes one phase's code instead of both.
+// Every lane of the warp calls it; `live` is false for a lane without a
+// ray. Returns true when this lane's ray finished.
+template <int kMode, class Sc>
+__device__ __forceinline__ bool vote_units(const Sc& sc, bool live, TravState& st, TravCold& tc,
+                                           const uint2* snodes, int n_smem, DevErr* err,
+                                           TravCount& cnt, int units) {
+  bool finished = false;
+  for (int u = 0; u < units; ++u) {
+    const bool go = live && !finished;
+    const unsigned lm = __ballot_sync(kFull, go);
+    if (lm == 0) break;
+    const bool testing = go && st.phase == kStepTest;
+    const unsigned tm = __ballot_sync(kFull, testing);
+    const bool pick_test = 2 * __popc(tm) >= __popc(lm);
+    if (go && testing == pick_test)
+      finished = trav_step<false, kMode == kTravStepSmem>(sc, st, tc, snodes, n_smem, err, cnt);
+  }
+  return finished;
+}
+#endif
+
+// --- Camera rays of a launch's primary-pass entries (P.prim_*), shared by
+// k_primary and the k_isect launches that carry them.
+// Entry g: its slot and ray index within the job.
+__device__ __forceinline__ bool prim_locate(const EngineParams& P, int64_t g, int& slot,
+                                            int64_t& ray) {
+  const int e = find_prefix(P.prim_prefix, P.prim_n, g);
+  slot = P.prim_slot[e];
+  ray = g - P.prim_prefix[e] + (P.prim_first ? P.prim_first[e] : 0);
+  bool ok = true;
+  HPT_DCHECK(&P.ctrl->err, slot >= 0 && slot < P.num_slots, 201, slot, ok = false);
+  HPT_DCHECK(&P.ctrl->err, !ok || (ray >= 0 && ray < job_rays(P.jobs[slot])), 202, ray,
+             ok = false);
+  return ok;
+}
+
+// Starts the walk of the job's camera ray (set_viewdirs / set_viewdirs_vr,
+// kernel.cl:559-613).
+__device__ __forceinline__ void prim_init(const DevJob& J, int64_t ray, TravState& st,
+                                          TravCold& tc) {
+  const int x = (int)(ray % J.nx), y = (int)(ray / J.nx);
+  const f3 d = J.pano ? pano_dir(x, y, J.vr_x_shift, J.ny)
+                      : pinhole_dir(J.top, J.right, J.width, J.height, x, y, J.nx, J.ny);
+  trav_init(J.scene, Ray{mk(J.view_p[0], J.view_p[1], J.view_p[2]), d}, st, tc);
+}
+
+// A finished camera ray: its hit goes to the job's primary-hit cache; a
+// miss adds the background (kernel.cl:193-206: the first pass assigns
+// background * strength * sample_n with strength (1,1,1)).
+__device__ __forceinline__ void prim_finish(const EngineParams& P, int slot, int64_t ray,
+                                            const TravState& st, const TravCold& tc) {
+  const DevJob& J = P.jobs[slot];
+  if (st.best.rec >= 0) {
+    int k = atomicAdd(J.prim_count, 1);
+    HPT_DCHECK(&P.ctrl->err, k < job_rays(J), 203, k, k = -1);
+    if (k >= 0) {
+      float4* dst = reinterpret_cast<float4*>(J.prim) + 2 * (size_t)k;
+      dst[0] = make_float4(st.ray.d.x, st.ray.d.y, st.ray.d.z, __int_as_float((int)ray));
+      dst[1] = make_float4(__int_as_float(st.best.tri), st.best.t, __int_as_float(tc.best_node),
+                           0.f);
+    }
+  } else {
+    const f3 val = scale((float)J.spp, mul(mk(J.bg[0], J.bg[1], J.bg[2]), mk(1.f, 1.f, 1.f)));
+    flush_radiance(J, ray, val);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // kMode: traversal as in k_isect.
 template <int BS, int MINB, int kMode>
@@ -284,23 +358,10 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
       drained = (int64_t)base + __popc(idle) >= total;
       if (!active) {
         const int64_t g = (int64_t)base + __popc(idle & lanemask_lt());
-        if (g < total) {
-          const int e = find_prefix(P.prim_prefix, P.prim_n, g);
-          slot = P.prim_slot[e];
-          ray = g - P.prim_prefix[e] + (P.prim_first ? P.prim_first[e] : 0);
-          bool ok = true;
-          HPT_DCHECK(&c->err, slot >= 0 && slot < P.num_slots, 201, slot, ok = false);
-          HPT_DCHECK(&c->err, !ok || (ray >= 0 && ray < job_rays(P.jobs[slot])), 202, ray,
-                     ok = false);
-          if (ok) {
-            const DevJob& J = P.jobs[slot];
-            const int x = (int)(ray % J.nx), y = (int)(ray / J.nx);
-            const f3 d = J.pano ? pano_dir(x, y, J.vr_x_shift, J.ny)
-                                : pinhole_dir(J.top, J.right, J.width, J.height, x, y, J.nx, J.ny);
-            trav_init(J.scene, Ray{mk(J.view_p[0], J.view_p[1], J.view_p[2]), d}, st, tc);
-            active = true;
-            ++queries;
-          }
+        if (g < total && prim_locate(P, g, slot, ray)) {
+          prim_init(P.jobs[slot], ray, st, tc);
+          active = true;
+          ++queries;
         }
       }
     }
@@ -337,50 +398,39 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
       }
     }
     if (finished) {
-      const DevJob& J = P.jobs[slot];
-      if (st.best.rec >= 0) {
-        int k = atomicAdd(J.prim_count, 1);
-        HPT_DCHECK(&c->err, k < job_rays(J), 203, k, k = -1);
-        if (k >= 0) {
-          float4* dst = reinterpret_cast<float4*>(J.prim) + 2 * (size_t)k;
-          dst[0] = make_float4(st.ray.d.x, st.ray.d.y, st.ray.d.z, __int_as_float((int)ray));
-          dst[1] = make_float4(__int_as_float(st.best.tri), st.best.t,
-                               __int_as_float(tc.best_node), 0.f);
-        }
-      } else {
-        // kernel.cl:193-206: the first pass assigns background * strength *
-        // sample_n with strength (1,1,1).
-        const f3 val = scale((float)J.spp, mul(mk(J.bg[0], J.bg[1], J.bg[2]), mk(1.f, 1.f, 1.f)));
-        flush_radiance(J, ray, val);
-      }
+      prim_finish(P, slot, ray, st, tc);
       active = false;
     }
   }
   flush_counts(c, queries, cnt);
 }
 
-// Sets the path counts of the slots whose primary pass completed and grants
-// paths (one thread). A slot whose primary pass is still partial stays as
-// it was: inactive, or finished with nothing left to issue.
+// Sets the path count of primary-pass entry e's slot when the entry
+// completes its job's primary pass. A slot whose primary pass is still
+// partial stays as it was: inactive, or finished with nothing left to issue.
+__device__ void activate_slot(const EngineParams& P, int e) {
+  const int s = P.prim_slot[e];
+  HPT_DCHECK(&P.ctrl->err, s >= 0 && s < P.num_slots, 232, s, return);
+  if (P.prim_final && !P.prim_final[e]) return;
+  DevSlot& S = P.slots[s];
+  S.num_paths = (int64_t)(*P.jobs[s].prim_count) * P.jobs[s].spp;
+  S.cursor = 0;
+  S.done = 0;
+  S.queries = 0;
+  S.max_inflight = P.jobs[s].max_inflight;
+  S.alloc = 0;
+  S.active = 1;
+}
+
+// After k_primary: starts the paths of the slots whose primary pass
+// completed and grants paths (one thread).
 __global__ void k_admit(EngineParams P) {
 #ifdef HPT_DEVICE_CHECKS
   HPT_DCHECK(&P.ctrl->err, P.ctrl->chk_isect_done == P.prim_prefix[P.prim_n], 243,
              P.ctrl->chk_isect_done, (void)0);
   P.ctrl->chk_isect_done = 0;
 #endif
-  for (int e = 0; e < P.prim_n; ++e) {
-    const int s = P.prim_slot[e];
-    HPT_DCHECK(&P.ctrl->err, s >= 0 && s < P.num_slots, 232, s, continue);
-    if (P.prim_final && !P.prim_final[e]) continue;
-    DevSlot& S = P.slots[s];
-    S.num_paths = (int64_t)(*P.jobs[s].prim_count) * P.jobs[s].spp;
-    S.cursor = 0;
-    S.done = 0;
-    S.queries = 0;
-    S.max_inflight = P.jobs[s].max_inflight;
-    S.alloc = 0;
-    S.active = 1;
-  }
+  for (int e = 0; e < P.prim_n; ++e) activate_slot(P, e);
   P.ctrl->prim_head = 0;
   schedule(P);
 }
@@ -542,7 +592,11 @@ __global__ void __launch_bounds__(BS, MINB) k_shade(EngineParams P) {
 // independently), reading nodes from global memory only / also from the
 // shared-memory prefix; kTravLeaf: one leaf per lane per round with
 // trav_leaf.
-template <int BS, int MINB, int kMode>
+// kPrim: the launch also traces the camera rays of its primary-pass entries
+// (P.prim_*), after the queue's rays, and records them as k_primary does;
+// k_ctrl then starts the paths of the jobs whose primary pass completed.
+// A serving loop admits requests this way, with no launch of its own.
+template <int BS, int MINB, int kMode, bool kPrim = false>
 __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
   constexpr bool kStep = kMode != kTravLeaf;
   extern __shared__ uint2 snodes[];
@@ -550,6 +604,7 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
   const TravScene* scene_tab = stage_scenes(P, snodes);
   DevCtrl* c = P.ctrl;
   const int n = c->nR;
+  const int64_t total = kPrim ? (int64_t)n + P.prim_prefix[P.prim_n] : (int64_t)n;
   const int out_par = c->parity ^ 1;
   const int lane = threadIdx.x & 31;
   bool active = false;
@@ -559,7 +614,9 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
   TravCold& tc = cold_sh[threadIdx.x];
   TravCount& cnt = count_sh[threadIdx.x].c;
   cnt = TravCount{};
-  int item = 0;   // index in the intersect queue; the payload is reloaded at the end
+  // Index in the intersect queue (the payload is reloaded at the end); with
+  // kPrim, -1 - ray for a camera ray.
+  int item = 0;
   int slot = 0;
   uint32_t queries = 0;  // this lane's queries in this launch
   // As in k_primary: a warp that finds the queue exhausted stops refilling.
@@ -570,9 +627,18 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
       unsigned long long base = 0;
       if (lane == 0) base = atomicAdd(&c->isect_head, (unsigned long long)__popc(idle));
       base = __shfl_sync(kFull, base, 0);
-      drained = (int64_t)base + __popc(idle) >= n;
+      drained = (int64_t)base + __popc(idle) >= total;
       if (!active) {
         const int64_t i = (int64_t)base + __popc(idle & lanemask_lt());
+        if constexpr (kPrim) {
+          int64_t ray = 0;
+          if (i >= n && i < total && prim_locate(P, i - n, slot, ray)) {
+            prim_init(P.jobs[slot], ray, st, tc);
+            item = -1 - (int)ray;
+            active = true;
+            ++queries;
+          }
+        }
         if (i < n) {
           bool ok = true;
           HPT_DCHECK(&c->err, i < P.capacity, 221, i, ok = false);
@@ -593,6 +659,21 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
     }
     if (__ballot_sync(kFull, active) == 0) break;
     bool finished = false;
+#if HPT_PHASE_VOTE
+    if constexpr (kStep) {
+      if (P.uniform_scene)
+        finished = vote_units<kMode>(P.uscene, active, st, tc, snodes, n_smem, &c->err, cnt,
+                                     P.trav_steps);
+      else if (P.scene_table)
+        finished = vote_units<kMode>(scene_tab[slot], active, st, tc, snodes, n_smem, &c->err,
+                                     cnt, P.trav_steps);
+      else
+        finished = vote_units<kMode>(P.jobs[slot].scene, active, st, tc, snodes, n_smem, &c->err,
+                                     cnt, P.trav_steps);
+    } else if (active) {
+      finished = trav_leaf(P.jobs[slot].scene, st, tc, snodes, n_smem, &c->err, cnt);
+    }
+#else
     if (active) {
       if constexpr (kStep) {
         if (P.uniform_scene) {
@@ -623,7 +704,13 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
         finished = trav_leaf(P.jobs[slot].scene, st, tc, snodes, n_smem, &c->err, cnt);
       }
     }
-    const bool hit = finished && st.best.rec >= 0;
+#endif
+    // A camera ray (kPrim) goes to its job's primary-hit cache instead.
+    const bool queued = !kPrim || item >= 0;
+    if constexpr (kPrim) {
+      if (finished && !queued) prim_finish(P, slot, -1 - (int64_t)item, st, tc);
+    }
+    const bool hit = finished && queued && st.best.rec >= 0;
     const unsigned hm = __ballot_sync(kFull, hit);
     if (hm) {
       const int leader = __ffs(hm) - 1;
@@ -645,7 +732,7 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
         }
       }
     }
-    const bool missed = finished && !hit;
+    const bool missed = finished && queued && !hit;
     if (missed) {
       // kernel.cl:195-200: miss adds background * strength (sample_n = 1).
       const DevJob& J = P.jobs[slot];
@@ -671,8 +758,8 @@ __global__ void k_ctrl(EngineParams P) {
 #ifdef HPT_DEVICE_CHECKS
   HPT_DCHECK(&c->err, c->chk_shade_done == c->chk_shade_items, 241,
              (long long)c->chk_shade_items * 1000000 + c->chk_shade_done, (void)0);
-  HPT_DCHECK(&c->err, c->chk_isect_done == c->nR, 242,
-             (long long)c->nR * 1000000 + c->chk_isect_done, (void)0);
+  HPT_DCHECK(&c->err, c->chk_isect_done == c->nR + (P.prim_n ? P.prim_prefix[P.prim_n] : 0),
+             242, (long long)c->nR * 1000000 + c->chk_isect_done, (void)0);
   c->chk_shade_items = 0;
   c->chk_shade_done = 0;
   c->chk_isect_done = 0;
@@ -688,6 +775,8 @@ __global__ void k_ctrl(EngineParams P) {
   c->isect_head = 0;
   c->parity ^= 1;
   c->iterations += 1;
+  // Jobs whose primary pass the iteration's k_isect completed (kPrim).
+  for (int e = 0; e < P.prim_n; ++e) activate_slot(P, e);
   schedule(P);
 }
 
@@ -702,6 +791,7 @@ struct IsectVariant {
   void (*primary)(EngineParams);
   void (*primary_step)(EngineParams);
   void (*primary_step_smem)(EngineParams);
+  void (*isect_step_prim)(EngineParams);  // step-at-a-time with primary-pass entries
   // The kernel a launch with these tuning values uses (shared-node prefix
   // only when smem_nodes > 0).
   void (*isect_kernel(int trav_steps, int smem_nodes) const)(EngineParams) {
@@ -714,7 +804,7 @@ struct IsectVariant {
 #define HPT_ISECT_VARIANT(B, M)                                                       \
   {B, M, k_isect<B, M, kTravLeaf>, k_isect<B, M, kTravStep>,                          \
    k_isect<B, M, kTravStepSmem>, k_primary<B, M, kTravLeaf>, k_primary<B, M, kTravStep>, \
-   k_primary<B, M, kTravStepSmem>}
+   k_primary<B, M, kTravStepSmem>, k_isect<B, M, kTravStep, true>}
 const IsectVariant kIsectVariants[] = {
     HPT_ISECT_VARIANT(128, 5), HPT_ISECT_VARIANT(128, 6), HPT_ISECT_VARIANT(128, 7),
     HPT_ISECT_VARIANT(128, 8), HPT_ISECT_VARIANT(128, 9), HPT_ISECT_VARIANT(128, 10),
@@ -1307,6 +1397,110 @@ hpt_status Engine::set_order_async(const std::vector<int>& order) {
   return HPT_OK;
 }
 
+// Uploads n primary-pass entries through a staging set: each entry's job
+// into its slot, then the slot list, the ray-count prefix and, with
+// `first` / `fin`, the first rays and final flags.
+hpt_status Engine::stage_primary(StagingSet& st, int n, const int* slot_ids, const DevJob* jobs,
+                                 const int64_t* rays, const int64_t* first, const int* fin) {
+  if (n > slots_)
+    return fail(HPT_ERR_INVALID_ARGUMENT, "%d primary entries for %d slots", n, slots_);
+  for (int k = 0; k < n; ++k) {
+    if (slot_ids[k] < 0 || slot_ids[k] >= slots_)
+      return fail(HPT_ERR_INVALID_ARGUMENT, "slot %d out of range", slot_ids[k]);
+    st.jobs[k] = jobs[k];
+    HPT_CUDA(cudaMemcpyAsync(jobs_ + slot_ids[k], st.jobs + k, sizeof(DevJob),
+                             cudaMemcpyHostToDevice, stream));
+  }
+  st.i64[0] = 0;
+  // Staging layout: i32 [0, n) slots, [slots + 1, 2 slots + 2] order (see
+  // upload_order), [2 slots + 3, + n) final flags; i64 [0, n] prefix,
+  // [slots + 1, + n) first rays.
+  int32_t* sfin = st.i32 + 2 * slots_ + 3;
+  int64_t* sfst = st.i64 + slots_ + 1;
+  for (int k = 0; k < n; ++k) {
+    st.i32[k] = slot_ids[k];
+    st.i64[k + 1] = st.i64[k] + rays[k];
+    if (first) {
+      sfst[k] = first[k];
+      sfin[k] = fin[k];
+    }
+  }
+  HPT_CUDA(cudaMemcpyAsync(prim_slot_, st.i32, n * sizeof(int32_t), cudaMemcpyHostToDevice,
+                           stream));
+  HPT_CUDA(cudaMemcpyAsync(prim_prefix_, st.i64, (n + 1) * sizeof(int64_t),
+                           cudaMemcpyHostToDevice, stream));
+  if (first) {
+    HPT_CUDA(cudaMemcpyAsync(prim_first_, sfst, n * sizeof(int64_t), cudaMemcpyHostToDevice,
+                             stream));
+    HPT_CUDA(cudaMemcpyAsync(prim_final_, sfin, n * sizeof(int32_t), cudaMemcpyHostToDevice,
+                             stream));
+  }
+  return HPT_OK;
+}
+
+bool Engine::fused_primary() const { return tuning.trav_steps > 0; }
+
+hpt_status Engine::queue_primary(int slot, const DevJob& job, int64_t rays, int64_t first,
+                                 bool final_part) {
+  if (slot < 0 || slot >= slots_ || rays <= 0 || first < 0)
+    return fail(HPT_ERR_INVALID_ARGUMENT, "primary entry: slot %d, %lld rays from %lld", slot,
+                (long long)rays, (long long)first);
+  for (size_t k = 0; k < pend_slot_.size(); ++k) {
+    if (pend_slot_[k] != slot) continue;
+    // A later part of the same job, queued before an iteration carried the
+    // earlier one: extend that entry.
+    if (pend_final_[k] || first != pend_first_[k] + pend_rays_[k])
+      return fail(HPT_ERR_INVALID_ARGUMENT, "primary parts of slot %d out of order", slot);
+    pend_rays_[k] += rays;
+    pend_final_[k] = final_part ? 1 : 0;
+    pend_job_[k] = job;
+    return HPT_OK;
+  }
+  pend_slot_.push_back(slot);
+  pend_job_.push_back(job);
+  pend_rays_.push_back(rays);
+  pend_first_.push_back(first);
+  pend_final_.push_back(final_part ? 1 : 0);
+  return HPT_OK;
+}
+
+hpt_status Engine::launch_iteration_async() {
+  const int n = (int)pend_slot_.size();
+  if (n == 0) {
+    launch_iteration(nullptr);
+    return HPT_OK;
+  }
+  if (!fused_primary())
+    return fail(HPT_ERR_INVALID_ARGUMENT, "queued primary rays need step-at-a-time traversal");
+  hpt_status s = query_occupancy();
+  if (s != HPT_OK) return s;
+  StagingSet* st = nullptr;
+  s = next_staging(&st);
+  if (s != HPT_OK) return s;
+  s = stage_primary(*st, n, pend_slot_.data(), pend_job_.data(), pend_rays_.data(),
+                    pend_first_.data(), pend_final_.data());
+  if (s != HPT_OK) return s;
+  HPT_CUDA(cudaEventRecord(st->ev, stream));
+  pend_slot_.clear();
+  pend_job_.clear();
+  pend_rays_.clear();
+  pend_first_.clear();
+  pend_final_.clear();
+  float4* A[8] = {A_o_[0], A_d_[0], A_s_[0], A_r_[0], A_o_[1], A_d_[1], A_s_[1], A_r_[1]};
+  float4* R[4] = {R_o_, R_d_, R_s_, R_r_};
+  EngineParams P = make_params(*this, ctrl_, jobs_, slot_state_, slots_, order_, quota_slot_,
+                               quota_prefix_, prim_slot_, prim_prefix_, n, capacity_, A, A_tri_,
+                               A_leaf_, R, nullptr);
+  P.prim_first = prim_first_;
+  P.prim_final = prim_final_;
+  shade_kernel(tuning)<<<num_sms * occ_shade_, 256, 0, stream>>>(P);
+  const IsectVariant& v = kIsectVariants[isect_variant()];
+  v.isect_step_prim<<<num_sms * occ_isect_, v.block, launch_smem(P), stream>>>(P);
+  k_ctrl<<<1, 1, 0, stream>>>(P);
+  HPT_CUDA(cudaGetLastError());
+  return HPT_OK;
+}
+
 hpt_status Engine::admit_async(const std::vector<int>& slot_ids, const std::vector<DevJob>& jobs,
                                const std::vector<int64_t>& rays, const std::vector<int>& order,
                                const DevScene* shared_scene, const std::vector<int64_t>& first,
@@ -1315,44 +1509,16 @@ hpt_status Engine::admit_async(const std::vector<int>& slot_ids, const std::vect
   if (n == 0) return set_order_async(order);
   hpt_status s = query_occupancy();
   if (s != HPT_OK) return s;
-  StagingSet* st = nullptr;
-  s = next_staging(&st);
-  if (s != HPT_OK) return s;
-  for (int k = 0; k < n; ++k) {
-    if (slot_ids[k] < 0 || slot_ids[k] >= slots_)
-      return fail(HPT_ERR_INVALID_ARGUMENT, "slot %d out of range", slot_ids[k]);
-    st->jobs[k] = jobs[k];
-    HPT_CUDA(cudaMemcpyAsync(jobs_ + slot_ids[k], st->jobs + k, sizeof(DevJob),
-                             cudaMemcpyHostToDevice, stream));
-  }
   const bool parts = !first.empty();
   if (parts && ((int)first.size() != n || (int)final_part.size() != n))
     return fail(HPT_ERR_INVALID_ARGUMENT, "primary parts: %d entries, %d firsts, %d flags", n,
                 (int)first.size(), (int)final_part.size());
-  st->i64[0] = 0;
-  // Staging layout: i32 [0, n) slots, [slots + 1, 2 slots + 2] order (see
-  // upload_order), [2 slots + 3, + n) final flags; i64 [0, n] prefix,
-  // [slots + 1, + n) first rays.
-  int32_t* fin = st->i32 + 2 * slots_ + 3;
-  int64_t* fst = st->i64 + slots_ + 1;
-  for (int k = 0; k < n; ++k) {
-    st->i32[k] = slot_ids[k];
-    st->i64[k + 1] = st->i64[k] + rays[k];
-    if (parts) {
-      fst[k] = first[k];
-      fin[k] = final_part[k];
-    }
-  }
-  HPT_CUDA(cudaMemcpyAsync(prim_slot_, st->i32, n * sizeof(int32_t), cudaMemcpyHostToDevice,
-                           stream));
-  HPT_CUDA(cudaMemcpyAsync(prim_prefix_, st->i64, (n + 1) * sizeof(int64_t),
-                           cudaMemcpyHostToDevice, stream));
-  if (parts) {
-    HPT_CUDA(cudaMemcpyAsync(prim_first_, fst, n * sizeof(int64_t), cudaMemcpyHostToDevice,
-                             stream));
-    HPT_CUDA(cudaMemcpyAsync(prim_final_, fin, n * sizeof(int32_t), cudaMemcpyHostToDevice,
-                             stream));
-  }
+  StagingSet* st = nullptr;
+  s = next_staging(&st);
+  if (s != HPT_OK) return s;
+  s = stage_primary(*st, n, slot_ids.data(), jobs.data(), rays.data(),
+                    parts ? first.data() : nullptr, parts ? final_part.data() : nullptr);
+  if (s != HPT_OK) return s;
   s = upload_order(order, *st);
   if (s != HPT_OK) return s;
   HPT_CUDA(cudaEventRecord(st->ev, stream));

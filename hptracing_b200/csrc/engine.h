@@ -91,6 +91,17 @@ class Engine {
                          const DevScene* shared_scene, const std::vector<int64_t>& first = {},
                          const std::vector<int>& final_part = {});
   hpt_status set_order_async(const std::vector<int>& order);
+  // Serving loop: a newly admitted job's camera rays can instead be traced
+  // inside the next iteration's traversal launch (fused_primary(): the
+  // tuning traverses step at a time), so that admissions add no launch of
+  // their own. queue_primary() records rays [first, first + rays) of the
+  // job in `slot` (parts of one job in order; final_part on the last, which
+  // starts its paths); launch_iteration_async() uploads what was queued and
+  // launches one iteration that carries it.
+  bool fused_primary() const;
+  hpt_status queue_primary(int slot, const DevJob& job, int64_t rays, int64_t first,
+                           bool final_part);
+  hpt_status launch_iteration_async();
   // Enqueues a copy of the slot table and control block into pinned host
   // memory and records ev after it.
   hpt_status read_state_async(DevSlot* slots, DevCtrl* ctrl, cudaEvent_t ev);
@@ -160,6 +171,11 @@ class Engine {
   int staging_next_ = 0, staging_slots_ = 0;
   hpt_status next_staging(StagingSet** out);
   hpt_status upload_order(const std::vector<int>& order, StagingSet& st);
+  hpt_status stage_primary(StagingSet& st, int n, const int* slot_ids, const DevJob* jobs,
+                           const int64_t* rays, const int64_t* first, const int* fin);
+  std::vector<int> pend_slot_, pend_final_;
+  std::vector<DevJob> pend_job_;
+  std::vector<int64_t> pend_rays_, pend_first_;
   cudaGraphExec_t graph_exec_ = nullptr;
   // The one scene the captured iterations were launched with (its pointers
   // and sizes are baked into the graph's kernel parameters), if any.

@@ -141,6 +141,8 @@ struct hpt_server {
   // finishes in time, so that about one in a hundred finishes late.
   double slack = 1.0;
   int64_t shed = 0;
+  // Camera rays of large requests queued since the last iteration launch.
+  int64_t large_queued = 0;
 
   double now_ms() const {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
@@ -222,15 +224,17 @@ hpt_status hpt_server::admit_pending() {
   std::vector<int64_t> rays, first;
   std::vector<int> final_part;
   const double now = now_ms();
-  // A latency-bound request's primary pass is traced whole at admission.
-  // A large request's is traced in parts, at most its in-flight share of
-  // the wavefront (large_inflight_pct, else a quarter) of rays per pump for
-  // all large requests together: one panorama's 2M camera rays traced in
-  // one launch would stall every request in flight for milliseconds.
+  // A latency-bound request's camera rays are traced whole at admission. A
+  // large request's are traced in parts, at most its in-flight share of the
+  // wavefront (large_inflight_pct, else a quarter) of rays per iteration for
+  // all large requests together: one panorama's 2M camera rays traced at
+  // once would stall every request in flight for milliseconds. With
+  // step-at-a-time traversal the camera rays ride in the next iteration's
+  // traversal launch (no launch, and no launch tail, of their own).
   const int pct = cfg.large_inflight_pct;
   const int64_t share = pct > 0 && pct < 100 ? (int64_t)cfg.capacity * pct / 100
                                              : (int64_t)cfg.capacity / 4;
-  int64_t large_budget = std::max<int64_t>(1024, share);
+  int64_t large_budget = std::max<int64_t>(1024, share) - large_queued;
   auto enqueue_part = [&](Request* r) {
     const int64_t left = r->rays - r->prim_next;
     const int64_t n = r->small ? left : std::min(left, std::max<int64_t>(1024, large_budget));
@@ -243,7 +247,10 @@ hpt_status hpt_server::admit_pending() {
     final_part.push_back(last ? 1 : 0);
     // Read-backs count the request only once its paths exist.
     r->admit_seq = last ? launched : std::numeric_limits<uint64_t>::max();
-    if (!r->small) large_budget -= n;
+    if (!r->small) {
+      large_budget -= n;
+      large_queued += n;
+    }
   };
   {
     // Requests part-way through their primary pass, oldest first.
@@ -346,6 +353,15 @@ hpt_status hpt_server::admit_pending() {
     it = queue.erase(it);
   }
   if (ids.empty()) return HPT_OK;
+  if (engine->fused_primary()) {
+    for (size_t k = 0; k < ids.size(); ++k) {
+      const hpt_status s = engine->queue_primary(ids[k], jobs[k], rays[k], first[k],
+                                                 final_part[k] != 0);
+      if (s != HPT_OK) return s;
+    }
+    return engine->set_order_async(order());
+  }
+  large_queued = 0;  // traced right now by their own launch
   HPT_TRACE_BEGIN(admit_async);
   const hpt_status s = engine->admit_async(ids, jobs, rays, order(), nullptr, first, final_part);
   HPT_TRACE_END(admit_async);
@@ -581,7 +597,9 @@ hpt_status hpt_server_pump(hpt_server* server, int32_t max_iterations) {
   // 3. Keep up to `depth` iterations queued, each followed by a read-back.
   int n = 0;
   while (n < std::max(1, max_iterations) && S.rb_pending < S.depth && S.running()) {
-    S.engine->launch_iteration(nullptr);
+    s = S.engine->launch_iteration_async();
+    if (s != HPT_OK) return s;
+    S.large_queued = 0;
     ++S.launched;
     ++n;
     Readback& b = S.rb[S.rb_fill];
