@@ -122,15 +122,16 @@ struct hpt_server {
   std::vector<cudaEvent_t> event_pool;
   int64_t completed = 0;
   int64_t pumps = 0;
-  // Overload policy (cfg.deadline_ms > 0). Per scene, two service times of
-  // a latency-bound request, each an upper quantile of recent observations:
+  // Overload policy (cfg.deadline_ms > 0). Per scene and request size, two
+  // service times of a latency-bound request, each an upper quantile of
+  // recent observations:
   // `alone` = completion minus admission for one admitted while no other
   // latency-bound request was running, `gap` = completion minus the previous
   // latency-bound completion for one admitted behind others. -1 = not
   // measured yet.
   struct ServiceEstimate {
     double alone = -1, gap = -1;
-    bool probing = false;  // the first request of the scene is running
+    bool probing = false;  // the first request of this scene and size is running
   };
   std::vector<ServiceEstimate> est;
   double last_small_done_ms = 0;
@@ -178,9 +179,16 @@ struct hpt_server {
     for (auto& p : v) o.push_back(p.second);
     return o;
   }
-  ServiceEstimate& estimate(int scene) {
-    if ((int)est.size() <= scene) est.resize(scene + 1);
-    return est[scene];
+  // Estimates are kept per scene and per request size (paths = rays x
+  // spp, by power of two): a 128x128 1-spp request says little about a
+  // 512x512 4-spp one on the same scene.
+  ServiceEstimate& estimate(const Request* r) {
+    const int64_t paths = std::max<int64_t>(1, r->rays * r->js.params.sample);
+    int bucket = 0;
+    while (bucket < 62 && ((int64_t)1 << (bucket + 1)) <= paths) ++bucket;
+    const size_t key = (size_t)r->scene_slot * 64 + bucket;
+    if (est.size() <= key) est.resize(key + 1);
+    return est[key];
   }
   // Latency-bound requests admitted and not yet retired.
   bool small_running() const {
@@ -285,7 +293,7 @@ hpt_status hpt_server::admit_pending() {
       // fit or are shed.
       const double waited = now - r->submit_ms;
       const double target = slack * cfg.deadline_ms;
-      ServiceEstimate& e = estimate(r->scene_slot);
+      ServiceEstimate& e = estimate(r);
       if (waited > cfg.deadline_ms || (e.alone >= 0 && waited + e.alone > target)) {
         // A stale estimate would shed this scene's requests for good:
         // every shed lowers it a little so that one is measured again.
@@ -340,7 +348,7 @@ hpt_status hpt_server::admit_pending() {
       r->drift_ms = drift_ms;
       r->alone = !busy;
       if (due >= 0) tail_ms = busy ? std::max(tail_ms, due) : due;
-      if (due < 0) estimate(r->scene_slot).probing = true;
+      if (due < 0) estimate(r).probing = true;
       busy = true;
     }
     slot_req[slot] = r->id;
@@ -443,13 +451,13 @@ hpt_status hpt_server::retire_finished() {
     r->done_ms = now_ms();
     finished_ids.push_back(r->id);
     ++completed;
-    if (r->small && cfg.deadline_ms > 0) estimate(r->scene_slot).probing = false;
+    if (r->small && cfg.deadline_ms > 0) estimate(r).probing = false;
     if (r->small && !r->cancel && cfg.deadline_ms > 0) {
       // Upper-quantile running estimates: quick to rise, slow to fall.
       auto track = [](double& q, double x) {
         q = q < 0 ? x : q + (x > q ? 0.25 : 0.05) * (x - q);
       };
-      ServiceEstimate& e = estimate(r->scene_slot);
+      ServiceEstimate& e = estimate(r);
       if (r->alone || e.alone < 0)
         track(e.alone, r->done_ms - r->admit_ms);
       else
