@@ -247,44 +247,53 @@ __global__ void __launch_bounds__(kCompactThreads)
   }
 }
 
-// One tile per block. Mask bits of flags at or past n are zero (the count
-// pass bounds-checks), so the scatter needs no n. The block of the last
-// tile writes the survivor total.
+// One tile per block, no staging: the 16-bit masks of lanes 2r and 2r + 1
+// of a warp, read as one 32-bit word, are the survivor bits of the 32
+// consecutive flags w * 512 + r * 32 + [0, 32) of its tile, lane l's flag
+// in bit l. So for each of its 16 rows a warp writes the row's survivors
+// to consecutive slots with one coalesced store (position: the popcount of
+// the row's bits below the lane). Mask bits of flags at or past n are zero
+// (the count pass bounds-checks), so the scatter needs no n. The block of
+// the last tile writes the survivor total.
 __global__ void __launch_bounds__(kCompactThreads)
-    k_compact_scatter(const uint16_t* masks, int tiles, int shift, const int* tile_counts,
+    k_compact_scatter(const uint32_t* rows, int tiles, int shift, const int* tile_counts,
                       const int* super_counts, int* out, int* total) {
-  __shared__ int staged[kCompactTile];
-  __shared__ int tile_count;
-  __shared__ int before[kCompactThreads / 32];
+  constexpr int kWarps = kCompactThreads / 32;
+  constexpr int kRows = kCompactItems;  // 32-flag rows per warp
+  __shared__ int before[kWarps], warp_count[kWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int b = blockIdx.x;
-  const uint32_t m = masks[(int64_t)b * kCompactThreads + threadIdx.x];
+  const uint32_t word = lane < kRows ? rows[((int64_t)b * kWarps + warp) * kRows + lane] : 0u;
+  const int wcount = __reduce_add_sync(0xFFFFFFFFu, __popc(word));
   // Survivors of the earlier superblocks, then of this superblock's earlier
-  // tiles.
+  // tiles (each warp sums a share).
   const int sb = b >> shift;
   int acc = 0;
   for (int i = threadIdx.x; i < sb; i += kCompactThreads) acc += super_counts[i];
   for (int i = (sb << shift) + threadIdx.x; i < b; i += kCompactThreads) acc += tile_counts[i];
   acc = __reduce_add_sync(0xFFFFFFFFu, acc);
-  if (lane == 0) before[warp] = acc;
-  // (The scan's barriers also publish before[] and tile_count.)
-  int pos = block_exclusive_scan<kCompactThreads>(__popc(m), &tile_count);
-  // Survivor indices of the tile in order, staged in shared memory (one
-  // predicated store per flag, no loop over set bits) ...
-  const int i0 = (int)((int64_t)b * kCompactTile) + (int)threadIdx.x * kCompactItems;
-#pragma unroll
-  for (int k = 0; k < kCompactItems; ++k) {
-    const int bit = (m >> k) & 1;
-    if (bit) staged[pos] = i0 + k;
-    pos += bit;
+  if (lane == 0) {
+    before[warp] = acc;
+    warp_count[warp] = wcount;
   }
-  int base = 0;
-#pragma unroll
-  for (int k = 0; k < kCompactThreads / 32; ++k) base += before[k];
   __syncthreads();
-  // ... then written out with consecutive threads on consecutive slots.
-  for (int k = threadIdx.x; k < tile_count; k += kCompactThreads) out[base + k] = staged[k];
-  if (b == tiles - 1 && threadIdx.x == 0) *total = base + tile_count;
+  int base = 0, offset = 0, count = 0;
+#pragma unroll
+  for (int k = 0; k < kWarps; ++k) {
+    base += before[k];
+    offset += k < warp ? warp_count[k] : 0;
+    count += warp_count[k];
+  }
+  int o = base + offset;
+  const int f0 = (int)((int64_t)b * kCompactTile) + warp * (kRows * 32) + lane;
+  const uint32_t below = (1u << lane) - 1u;  // lanes below this one
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+    const uint32_t bits = __shfl_sync(0xFFFFFFFFu, word, r);
+    if ((bits >> lane) & 1u) out[o + __popc(bits & below)] = f0 + r * 32;
+    o += __popc(bits);
+  }
+  if (b == tiles - 1 && threadIdx.x == 0) *total = base + count;
 }
 
 inline int blocks_for(int64_t n, int bs) { return (int)((n + bs - 1) / bs); }
@@ -301,8 +310,9 @@ cudaError_t launch_compact(const uint32_t* flags, int n, int* tile_counts, int* 
   if (e != cudaSuccess) return e;
   k_compact_count<<<tiles, kCompactThreads, 0, st>>>(flags, n, shift, tile_counts, super_counts,
                                                      masks);
-  k_compact_scatter<<<tiles, kCompactThreads, 0, st>>>(masks, tiles, shift, tile_counts,
-                                                       super_counts, out, total);
+  k_compact_scatter<<<tiles, kCompactThreads, 0, st>>>(reinterpret_cast<const uint32_t*>(masks),
+                                                       tiles, shift, tile_counts, super_counts,
+                                                       out, total);
   return cudaGetLastError();
 }
 
