@@ -354,19 +354,19 @@ hpt_status hpt_compact(const uint32_t* flags, int32_t n, int32_t* out,
  * out and count are device pointers; the work is enqueued on `stream`
  * (a cudaStream_t, NULL = legacy default stream) and the call returns
  * without waiting: *count is valid once the stream reaches that point.
- * The scratch (tile counts, superblock totals, one mask byte per 8 flags:
+ * The scratch (tile counts, superblock totals, one mask bit per flag:
  * 4.1 MiB) is fixed static device arrays, so n is limited to
  * HPT_COMPACT_NOALLOC_MAX_N flags (larger n: HPT_ERR_INVALID_ARGUMENT,
  * nothing enqueued). The first call on each device looks up those arrays'
- * addresses (set-up, with the device current); make that first call before
- * any stream capture. Every call shares the one set of arrays: calls whose
+ * addresses (set-up, with the device current). Every call shares the one
+ * set of arrays: calls whose
  * work overlaps on the GPU (different streams, or host threads) race on it
  * and must be serialised by the caller. Each call overwrites (or zeroes,
  * with cudaMemsetAsync on `stream`) every scratch entry it reads, so no
  * state carries over between calls. The addresses are cached per device:
  * after cudaDeviceReset this entry point must not be called again in the
  * same process. */
-#define HPT_COMPACT_NOALLOC_MAX_N (16384 * 2048)
+#define HPT_COMPACT_NOALLOC_MAX_N (8192 * 4096)
 hpt_status hpt_compact_noalloc(const uint32_t* flags, int32_t n,
                                int32_t* out, int32_t* count, void* stream);
 

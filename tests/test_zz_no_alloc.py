@@ -19,14 +19,15 @@ def torch_cuda(built):
     return torch
 
 
-def _noalloc(torch, flags):
-    """Runs hpt_compact_noalloc on device copies of flags; returns
-    (status, count, indices)."""
+def _noalloc(torch, flags, stream=None):
+    """Runs hpt_compact_noalloc on device copies of flags (on `stream`, else
+    torch's current stream); returns (status, count, indices)."""
     n = len(flags)
     d_flags = torch.from_numpy(flags.view(np.int32)).cuda()
     d_out = torch.full((max(n, 1),), -1, dtype=torch.int32, device="cuda")
     d_count = torch.full((1,), -1, dtype=torch.int32, device="cuda")
-    stream = torch.cuda.current_stream()
+    stream = stream or torch.cuda.current_stream()
+    stream.wait_stream(torch.cuda.current_stream())  # inputs written on the current stream
     st = H.lib().hpt_compact_noalloc(d_flags.data_ptr(), n, d_out.data_ptr(),
                                      d_count.data_ptr(), stream.cuda_stream)
     stream.synchronize()
@@ -47,9 +48,23 @@ def test_noalloc_matches_compact_on_consecutive_calls(torch_cuda):
         assert np.array_equal(got, want)
 
 
+def test_noalloc_on_a_side_stream(torch_cuda):
+    """The work is enqueued on the caller's stream: on a side stream, at the
+    limit size and at a ragged one, the results equal hpt_compact's."""
+    rng = np.random.default_rng(12)
+    side = torch_cuda.cuda.Stream()
+    for n, density in ((8192 * 4096, 0.5), (4097, 0.02)):
+        flags = (rng.random(n) < density).astype(np.uint32)
+        want = H.compact(flags)
+        st, count, got = _noalloc(torch_cuda, flags, side)
+        assert st == 0, H.lib().hpt_last_error()
+        assert count == len(want)
+        assert np.array_equal(got, want)
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch(torch_cuda):
     L = H.lib()
-    limit = 16384 * 2048
+    limit = 8192 * 4096
     d = torch_cuda.zeros(1, dtype=torch_cuda.int32, device="cuda")
     st = L.hpt_compact_noalloc(d.data_ptr(), limit + 1, d.data_ptr(), d.data_ptr(), None)
     assert st == 1
