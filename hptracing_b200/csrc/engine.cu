@@ -928,8 +928,10 @@ hpt_tuning default_tuning() {
   hpt_tuning t;
   memset(&t, 0, sizeof t);
   // From the tuning sweeps on the 61k-triangle spheres frame (512x512,
-  // 64 spp) and the 2.4M-triangle terrain frame: step-at-a-time traversal,
-  // 24 units per refill check, 10 blocks of 128 per SM (48 registers; the
+  // 64 spp) and the 2.4M-triangle terrain frame: step-at-a-time traversal
+  // with the phase vote, 48 warp rounds per refill check (16 / 24 / 32 /
+  // 48: spheres 107.0 / 105.7 / 105.0 / 105.0 ms, terrain at 4 spp 79.6 /
+  // 79.0 / 78.7 / 77.7 ms), 10 blocks of 128 per SM (48 registers; the
   // per-leaf state and counters live in shared memory), no shared-node
   // prefix.
   t.capacity = 1 << 22;
@@ -939,7 +941,7 @@ hpt_tuning default_tuning() {
   t.refill_chunk = 4;
   t.smem_nodes = 0;
   t.use_graph = 0;
-  t.trav_steps = 24;
+  t.trav_steps = 48;
   // Shading at 4 blocks of 256 per SM (64 registers): 7.0 instead of 8.4 ms
   // per spheres frame at the natural 106-register allocation (2 blocks).
   t.shade_min_blocks = 4;

@@ -24,6 +24,7 @@
 #include <cstring>
 #include <deque>
 #include <fstream>
+#include <iterator>
 #include <limits>
 #include <map>
 #include <memory>
@@ -119,6 +120,12 @@ struct hpt_server {
   DevCtrl ctrl_view{};
   std::vector<uint64_t> finished_ids;  // since the last hpt_server_drain_completed
   std::multimap<size_t, void*> pinned_pool;  // free pinned output buffers by size
+  // Pinned host memory for results, pinned at creation (cudaMallocHost in
+  // the middle of a stream stalls the pump for milliseconds): a first-fit
+  // arena in 4 KB units; cudaMallocHost only once it is full.
+  uint8_t* arena = nullptr;
+  size_t arena_bytes = 0;
+  std::map<size_t, size_t> arena_free;  // offset -> length of each free range
   std::vector<cudaEvent_t> event_pool;
   int64_t completed = 0;
   int64_t pumps = 0;
@@ -196,7 +203,20 @@ struct hpt_server {
       if (slot_req[k] && reqs.at(slot_req[k])->small) return true;
     return false;
   }
+  static size_t arena_units(size_t bytes) { return (bytes + 4095) & ~(size_t)4095; }
+  bool in_arena(const void* p) const {
+    return arena && p >= arena && static_cast<const uint8_t*>(p) < arena + arena_bytes;
+  }
   hpt_status take_pinned(size_t bytes, void** out) {
+    const size_t len = arena_units(bytes);
+    for (auto it = arena_free.begin(); it != arena_free.end(); ++it) {
+      if (it->second < len) continue;
+      const size_t off = it->first, rest = it->second - len;
+      arena_free.erase(it);
+      if (rest) arena_free[off + len] = rest;
+      *out = arena + off;
+      return HPT_OK;
+    }
     auto it = pinned_pool.find(bytes);
     if (it != pinned_pool.end()) {
       *out = it->second;
@@ -207,7 +227,28 @@ struct hpt_server {
     return HPT_OK;
   }
   void give_pinned(void* p, size_t bytes) {
-    if (p) pinned_pool.insert({bytes, p});
+    if (!p) return;
+    if (!in_arena(p)) {
+      pinned_pool.insert({bytes, p});
+      return;
+    }
+    size_t off = static_cast<uint8_t*>(p) - arena, len = arena_units(bytes);
+    auto next = arena_free.lower_bound(off);
+    if (next != arena_free.end() && next->first == off + len) {  // merge with the range after
+      len += next->second;
+      next = arena_free.erase(next);
+    }
+    if (next != arena_free.begin()) {  // and with the range before
+      auto prev = std::prev(next);
+      if (prev->first + prev->second == off) {
+        prev->second += len;
+        return;
+      }
+    }
+    arena_free[off] = len;
+  }
+  void free_pinned(void* p) {
+    if (p && !in_arena(p)) HPT_SOFT(cudaFreeHost(p));
   }
   hpt_status take_event(cudaEvent_t* ev) {
     if (!event_pool.empty()) {
@@ -519,6 +560,12 @@ hpt_status hpt_server_create(const hpt_server_config* config, hpt_server** out) 
     // for the driver to map memory.
     st = s->engine->reserve_pool((size_t)config->memory_budget);
     if (st != HPT_OK) return st;
+    s->arena_bytes = std::min<size_t>(512u << 20, std::max<size_t>(16u << 20,
+                                      (size_t)config->memory_budget / 16));
+    void* arena = nullptr;
+    HPT_CUDA(cudaMallocHost(&arena, s->arena_bytes));
+    s->arena = static_cast<uint8_t*>(arena);
+    s->arena_free[0] = s->arena_bytes;
     for (Readback& b : s->rb) {
       HPT_CUDA(cudaMallocHost(&b.slots, (size_t)config->max_jobs * sizeof(DevSlot)));
       HPT_CUDA(cudaMallocHost(&b.ctrl, sizeof(DevCtrl)));
@@ -757,8 +804,8 @@ void hpt_server_destroy(hpt_server* server) {
         Request* r = kv.second.get();
         if (r->slot >= 0) server->engine->free_job(r->buf);
         if (r->fin_ev) HPT_SOFT(cudaEventDestroy(r->fin_ev));
-        if (r->rgba) HPT_SOFT(cudaFreeHost(r->rgba));
-        if (r->accum) HPT_SOFT(cudaFreeHost(r->accum));
+        server->free_pinned(r->rgba);
+        server->free_pinned(r->accum);
       }
       HPT_SOFT(cudaStreamSynchronize(server->engine->stream));
     }
@@ -768,6 +815,7 @@ void hpt_server_destroy(hpt_server* server) {
       if (b.ev) HPT_SOFT(cudaEventDestroy(b.ev));
     }
     for (auto& kv : server->pinned_pool) HPT_SOFT(cudaFreeHost(kv.second));
+    if (server->arena) HPT_SOFT(cudaFreeHost(server->arena));
     for (cudaEvent_t e : server->event_pool) HPT_SOFT(cudaEventDestroy(e));
   }
   delete server;
@@ -882,7 +930,7 @@ extern "C" hpt_status hpt_autotune(hpt_scene* scene, const hpt_camera* camera,
          t.isect_block = a;
          t.isect_min_blocks = b;
        }},
-      {{{0, 0}, {8, 0}, {16, 0}, {32, 0}},
+      {{{0, 0}, {16, 0}, {32, 0}, {48, 0}},
        [](hpt_tuning& t, int a, int) { t.trav_steps = a; }},
       {{{2, 0}, {4, 0}, {8, 0}, {16, 0}},
        [](hpt_tuning& t, int a, int) { t.refill_chunk = a; }},
