@@ -33,6 +33,7 @@
 #include <cstring>
 #include <mutex>
 #include <numeric>
+#include <type_traits>
 
 #include "engine.h"
 #include "shading.cuh"
@@ -150,7 +151,7 @@ __device__ __forceinline__ void count_queries(DevSlot* slots, bool alive, int sl
 // traversal unit and would otherwise hold four registers.
 struct CountSlot {
   TravCount c;
-  uint32_t pad;
+  uint32_t queries;  // the lane's queries in this launch
 };
 
 // Warp-level reduction of the per-lane query and work counters.
@@ -262,18 +263,187 @@ constexpr int kTravStepSmem = 2;  // trav_step with the shared-memory node prefi
 #define HPT_PHASE_VOTE 1
 #endif
 // The tests' phase runs when it holds at least this many sixths of the
-// warp's live lanes (3: the majority).
+// warp's live lanes: with one test per testing lane a round (3, the
+// majority), and with cooperative tests (1; a cooperative round tests up to
+// 32 references whatever the number of testing lanes).
 #ifndef HPT_VOTE_TEST_SIXTHS
 #define HPT_VOTE_TEST_SIXTHS 3
 #endif
+#ifndef HPT_COOP_TEST_SIXTHS
+#define HPT_COOP_TEST_SIXTHS 1
+#endif
+// k_primary tests one reference per testing lane a round unless built with
+// -DHPT_COOP_PRIMARY=1: camera rays are coherent, neighbouring lanes test
+// the same triangles and share their loads, and the terrain frame's
+// primary pass measured 9.6 ms with per-lane tests against 11.3 ms with
+// cooperative ones (the spheres frame's 1.16 against 0.87 ms).
+#ifndef HPT_COOP_PRIMARY
+#define HPT_COOP_PRIMARY 0
+#endif
+constexpr bool kCoopPrimary = HPT_COOP_PRIMARY != 0;
+// Scene accessors of the traversal loops: scene_of(slot) is the scene of a
+// job slot's rays - the launch's one scene (kernel parameters), the
+// per-block table of a several-scene launch, or the job table.
+struct OneScene {
+  const DevScene& s;
+  __device__ __forceinline__ const DevScene& operator()(int) const { return s; }
+};
+struct TableScene {
+  const TravScene* tab;
+  __device__ __forceinline__ const TravScene& operator()(int slot) const { return tab[slot]; }
+};
+struct JobScene {
+  const DevJob* jobs;
+  __device__ __forceinline__ const DevScene& operator()(int slot) const {
+    return jobs[slot].scene;
+  }
+};
+
+// Warp-cooperative triangle tests (default with the phase vote;
+// -DHPT_COOP_TESTS=0 builds the one-test-per-lane rounds): in a test round
+// the untested references of every testing lane's current leaf are dealt
+// out over the warp's 32 lanes, one test per lane, and a segmented minimum
+// over (t, rank) hands each ray the best of its candidates. The reference's
+// rule - the smallest t wins, the lower rank on an exact tie - is a
+// lexicographic minimum, so the order in which the tests run does not
+// change any result.
+#ifndef HPT_COOP_TESTS
+#define HPT_COOP_TESTS 1
+#endif
+
 #if HPT_PHASE_VOTE
+#if HPT_COOP_TESTS
+// One cooperative test round; every lane of the warp calls it. `testing`:
+// this lane's ray is in the test phase; `slot`: its job slot, whose scene
+// scene_of(slot) gives (a lane may test for a ray of another job, so it
+// reads that ray's scene). Returns true when this lane's ray finished (its
+// leaf's last reference was tested and the exit ended it).
+template <class SceneOf>
+__device__ __forceinline__ bool coop_tests(const SceneOf& scene_of, int slot, bool testing,
+                                           TravState& st, TravCold& tc, DevErr* err,
+                                           TravCount& cnt) {
+  const int lane = threadIdx.x & 31;
+  const int rem = testing ? st.end - st.k : 0;
+  // This lane's references take slots [excl, incl) of the round.
+  int incl = rem;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int excl = incl - rem;
+  const int total = __shfl_sync(kFull, incl, 31);
+  // Slot `lane` belongs to the first lane whose inclusive end exceeds it.
+  int owner = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1) {
+    const int v = __shfl_sync(kFull, incl, owner + step - 1);
+    if (v <= lane) owner += step;
+  }
+  const bool valid = lane < total;
+  const int o_k = __shfl_sync(kFull, st.k, owner);
+  const int o_excl = __shfl_sync(kFull, excl, owner);
+  const int o_mb = __shfl_sync(kFull, st.mb_id[0], owner);
+  const int o_slot = __shfl_sync(kFull, slot, owner);
+#if HPT_RAY_IN_SMEM
+  // The owner's TravCold sits (owner - lane) entries away in the block's
+  // per-lane array.
+  const Ray r = (&tc)[owner - lane].ray;
+#else
+  Ray r;
+  r.o.x = __shfl_sync(kFull, st.ray.o.x, owner);
+  r.o.y = __shfl_sync(kFull, st.ray.o.y, owner);
+  r.o.z = __shfl_sync(kFull, st.ray.o.z, owner);
+  r.d.x = __shfl_sync(kFull, st.ray.d.x, owner);
+  r.d.y = __shfl_sync(kFull, st.ray.d.y, owner);
+  r.d.z = __shfl_sync(kFull, st.ray.d.z, owner);
+#endif
+  int id = -1;
+  uint32_t key = ~0u;  // t's bits for a hit (t > 0: ordered like t), else the maximum
+  if (valid) {
+    const auto& so = scene_of(o_slot);
+    const int j = o_k + (lane - o_excl);
+    bool ok = true;
+    HPT_DCHECK(err, j >= 0 && j < so.num_leaf_tris, 107, j, ok = false);
+    if (ok) {
+      id = ldg(so.leaf_refs + j);
+      HPT_DCHECK(err, id >= 0 && id < so.num_triangles, 104, id, ok = false);
+    }
+    if (ok) {
+      const float4* rec = reinterpret_cast<const float4*>(so.tris) + 3 * (size_t)id;
+      float t, u, v;
+      if (mt_test(r, ldg(rec), ldg(rec + 1), ldg(rec + 2), t, u, v)) key = __float_as_uint(t);
+    }
+  }
+  // Work counters as the one-test-per-lane walk counts them: a reference
+  // equal to the one before it in its ray's sequence is a mailbox repeat.
+  const int up = __shfl_up_sync(kFull, id, 1);
+  if (valid) {
+    if (id == (lane == o_excl ? o_mb : up)) ++cnt.repeats;
+    else ++cnt.tris;
+  }
+  // Segmented minimum of t: the first slot of each ray's range ends with
+  // its range's minimum. Bit s of `starts`: slot s begins a range.
+  const unsigned starts = __ballot_sync(kFull, valid && lane == o_excl);
+  const uint32_t mine = key;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t other = __shfl_down_sync(kFull, key, o);
+    const bool same =
+        lane + o < 32 &&
+        ((unsigned)((unsigned long long)starts >> (lane + 1)) & ((1u << o) - 1)) == 0;
+    if (same && other < key) key = other;
+  }
+  // Of the slots that hold their range's minimum the lowest one - the
+  // lowest rank - wins, as the reference's strict comparison in list order
+  // keeps the first of equal t.
+  const uint32_t seg_min = __shfl_sync(kFull, key, o_excl);
+  const unsigned wins = __ballot_sync(kFull, valid && mine != ~0u && mine == seg_min);
+  const int first = excl < 32 ? excl : 31;
+  const int last = incl < 32 ? incl - 1 : 31;
+  const unsigned my_wins = (unsigned)(((unsigned long long)wins >> first) << first);
+  const int w = my_wins ? __ffs(my_wins) - 1 : 0;
+  const int last_id = __shfl_sync(kFull, id, last < 0 ? 0 : last);
+  const int win_id = __shfl_sync(kFull, id, w);
+  const uint32_t best = __shfl_sync(kFull, key, first);
+  if (!testing) return false;
+  if (rem > 0 && excl < 32) {
+    const int k0 = st.k;
+    st.k += last + 1 - excl;
+    st.mb_id[0] = last_id;
+    // When the range holds a hit, w is its lowest slot at the range's
+    // minimum (the slots past the range belong to other rays).
+    if (best != ~0u && w <= last) {
+      const float t = __uint_as_float(best);
+      const int jb = k0 + (w - excl);
+      if (st.best.rec < 0 || t < st.best.t || (t == st.best.t && jb < st.best.rec)) {
+        const auto& s = scene_of(slot);
+        if (tc.pierced < 0) {
+          const float4* L = reinterpret_cast<const float4*>(s.leaves + tc.leaf);
+          tc.pierced = ref_box_test(ray_of(st, tc), ldg(L), ldg(L + 1)) ? 1 : 0;
+        }
+        if (tc.pierced) {
+          st.best.rec = jb;
+          st.best.tri = win_id;
+          st.best.t = t;
+          tc.best_node = tc.leaf_node;
+        }
+      }
+    }
+  }
+  if (st.k < st.end) return false;
+  return trav_exit(scene_of(slot), st, tc, err);
+}
+#endif
+
 // Up to `units` warp rounds. Every lane of the warp calls it; `live` is
-// false for a lane without a ray. Returns true when this lane's ray
-// finished.
-template <int kMode, class Sc>
-__device__ __forceinline__ bool vote_units(const Sc& sc, bool live, TravState& st, TravCold& tc,
-                                           const uint2* snodes, int n_smem, DevErr* err,
-                                           TravCount& cnt, int units) {
+// false for a lane without a ray; scene_of(slot) is the scene of this
+// lane's job. kCoop: test rounds are cooperative (coop_tests). Returns true
+// when this lane's ray finished.
+template <int kMode, bool kCoop, class SceneOf>
+__device__ __forceinline__ bool vote_units(const SceneOf& scene_of, int slot, bool live,
+                                           TravState& st, TravCold& tc, const uint2* snodes,
+                                           int n_smem, DevErr* err, TravCount& cnt, int units) {
   bool finished = false;
   for (int u = 0; u < units; ++u) {
     const bool go = live && !finished;
@@ -281,9 +451,24 @@ __device__ __forceinline__ bool vote_units(const Sc& sc, bool live, TravState& s
     if (lm == 0) break;
     const bool testing = go && st.phase == kStepTest;
     const unsigned tm = __ballot_sync(kFull, testing);
+#if HPT_COOP_TESTS
+    if constexpr (kCoop) {
+      // Every round moves a lane on: a test round needs a testing lane
+      // (whatever the threshold), else the descending lanes run.
+      if (tm != 0 && 6 * __popc(tm) >= HPT_COOP_TEST_SIXTHS * __popc(lm)) {
+        if (coop_tests(scene_of, slot, testing, st, tc, err, cnt)) finished = true;
+      } else if (go && !testing) {
+        finished = trav_step<false, kMode == kTravStepSmem,
+                             std::decay_t<decltype(scene_of(slot))>, false>(
+            scene_of(slot), st, tc, snodes, n_smem, err, cnt);
+      }
+      continue;
+    }
+#endif
     const bool pick_test = 6 * __popc(tm) >= HPT_VOTE_TEST_SIXTHS * __popc(lm);
     if (go && testing == pick_test)
-      finished = trav_step<false, kMode == kTravStepSmem>(sc, st, tc, snodes, n_smem, err, cnt);
+      finished = trav_step<false, kMode == kTravStepSmem>(scene_of(slot), st, tc, snodes, n_smem,
+                                                          err, cnt);
   }
   return finished;
 }
@@ -325,7 +510,8 @@ __device__ __forceinline__ void prim_finish(const EngineParams& P, int slot, int
     HPT_DCHECK(&P.ctrl->err, k < job_rays(J), 203, k, k = -1);
     if (k >= 0) {
       float4* dst = reinterpret_cast<float4*>(J.prim) + 2 * (size_t)k;
-      dst[0] = make_float4(st.ray.d.x, st.ray.d.y, st.ray.d.z, __int_as_float((int)ray));
+      const f3 d = ray_of(st, tc).d;
+      dst[0] = make_float4(d.x, d.y, d.z, __int_as_float((int)ray));
       dst[1] = make_float4(__int_as_float(st.best.tri), st.best.t, __int_as_float(tc.best_node),
                            0.f);
     }
@@ -353,9 +539,14 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
   TravCold& tc = cold_sh[threadIdx.x];
   TravCount& cnt = count_sh[threadIdx.x].c;
   cnt = TravCount{};
+  uint32_t& queries = count_sh[threadIdx.x].queries;
+  queries = 0;
   int slot = 0;
-  int64_t ray = 0;
-  uint32_t queries = 0;  // this lane's queries in this launch
+  // The lane's camera ray (read when it finishes; shared memory keeps the
+  // registers for the traversal).
+  __shared__ int64_t ray_sh[BS];
+  int64_t& ray = ray_sh[threadIdx.x];
+  ray = 0;
   // Once a refill finds the rays exhausted the warp stops asking (the value
   // is warp-uniform), so the cursor overshoots by at most one grab per warp.
   bool drained = false;
@@ -380,14 +571,14 @@ __global__ void __launch_bounds__(BS, MINB) k_primary(EngineParams P) {
 #if HPT_PHASE_VOTE
     if constexpr (kStep) {
       if (P.uniform_scene)
-        finished = vote_units<kMode>(P.uscene, active, st, tc, snodes, n_smem, &c->err, cnt,
-                                     P.trav_steps);
+        finished = vote_units<kMode, kCoopPrimary>(OneScene{P.uscene}, slot, active, st, tc,
+                                         snodes, n_smem, &c->err, cnt, P.trav_steps);
       else if (P.scene_table)
-        finished = vote_units<kMode>(scene_tab[slot], active, st, tc, snodes, n_smem, &c->err,
-                                     cnt, P.trav_steps);
+        finished = vote_units<kMode, kCoopPrimary>(TableScene{scene_tab}, slot, active, st, tc,
+                                         snodes, n_smem, &c->err, cnt, P.trav_steps);
       else
-        finished = vote_units<kMode>(P.jobs[slot].scene, active, st, tc, snodes, n_smem, &c->err,
-                                     cnt, P.trav_steps);
+        finished = vote_units<kMode, kCoopPrimary>(JobScene{P.jobs}, slot, active, st, tc,
+                                         snodes, n_smem, &c->err, cnt, P.trav_steps);
     } else if (active) {
       finished = trav_leaf(P.jobs[slot].scene, st, tc, snodes, n_smem, &c->err, cnt);
     }
@@ -640,11 +831,15 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
   TravCold& tc = cold_sh[threadIdx.x];
   TravCount& cnt = count_sh[threadIdx.x].c;
   cnt = TravCount{};
+  uint32_t& queries = count_sh[threadIdx.x].queries;
+  queries = 0;
   // Index in the intersect queue (the payload is reloaded at the end); with
-  // kPrim, -1 - ray for a camera ray.
-  int item = 0;
+  // kPrim, -1 - ray for a camera ray. Read when the ray finishes, so it
+  // stays in shared memory.
+  __shared__ int item_sh[BS];
+  int& item = item_sh[threadIdx.x];
+  item = 0;
   int slot = 0;
-  uint32_t queries = 0;  // this lane's queries in this launch
   // As in k_primary: a warp that finds the queue exhausted stops refilling.
   bool drained = false;
   while (true) {
@@ -688,14 +883,14 @@ __global__ void __launch_bounds__(BS, MINB) k_isect(EngineParams P) {
 #if HPT_PHASE_VOTE
     if constexpr (kStep) {
       if (P.uniform_scene)
-        finished = vote_units<kMode>(P.uscene, active, st, tc, snodes, n_smem, &c->err, cnt,
-                                     P.trav_steps);
+        finished = vote_units<kMode, true>(OneScene{P.uscene}, slot, active, st, tc,
+                                         snodes, n_smem, &c->err, cnt, P.trav_steps);
       else if (P.scene_table)
-        finished = vote_units<kMode>(scene_tab[slot], active, st, tc, snodes, n_smem, &c->err,
-                                     cnt, P.trav_steps);
+        finished = vote_units<kMode, true>(TableScene{scene_tab}, slot, active, st, tc,
+                                         snodes, n_smem, &c->err, cnt, P.trav_steps);
       else
-        finished = vote_units<kMode>(P.jobs[slot].scene, active, st, tc, snodes, n_smem, &c->err,
-                                     cnt, P.trav_steps);
+        finished = vote_units<kMode, true>(JobScene{P.jobs}, slot, active, st, tc,
+                                         snodes, n_smem, &c->err, cnt, P.trav_steps);
     } else if (active) {
       finished = trav_leaf(P.jobs[slot].scene, st, tc, snodes, n_smem, &c->err, cnt);
     }
@@ -931,12 +1126,14 @@ hpt_tuning default_tuning() {
   // 64 spp) and the 2.4M-triangle terrain frame: step-at-a-time traversal
   // with the phase vote, 48 warp rounds per refill check (16 / 24 / 32 /
   // 48: spheres 107.0 / 105.7 / 105.0 / 105.0 ms, terrain at 4 spp 79.6 /
-  // 79.0 / 78.7 / 77.7 ms), 10 blocks of 128 per SM (48 registers; the
-  // per-leaf state and counters live in shared memory), no shared-node
-  // prefix.
+  // 79.0 / 78.7 / 77.7 ms; with cooperative tests 32 / 48 / 64: 92.5 /
+  // 92.3 / 93.0 ms), 9 blocks of 128 per SM (56 registers; with
+  // cooperative tests 8 / 9 / 10 blocks: spheres 94.8 / 92.3 / 101.4 ms,
+  // terrain 74.3 / 70.7 / 81.5 ms - at 10 the 48-register budget spills),
+  // no shared-node prefix.
   t.capacity = 1 << 22;
   t.isect_block = 128;
-  t.isect_min_blocks = 10;
+  t.isect_min_blocks = 9;
   t.shade_block = 256;
   t.refill_chunk = 4;
   t.smem_nodes = 0;

@@ -86,10 +86,19 @@ constexpr int kMailbox = HPT_MAILBOX;
 constexpr int32_t kStepDescend = 0;
 constexpr int32_t kStepTest = 1;
 
+// Where a walking ray's origin and direction live: in TravState (registers)
+// or, built with -DHPT_RAY_IN_SMEM=1, in TravCold (shared memory in the
+// kernels), which frees six registers per lane.
+#ifndef HPT_RAY_IN_SMEM
+#define HPT_RAY_IN_SMEM 0
+#endif
+
 // Traversal state of one ray that most units touch; lives in registers so
 // a lane can be refilled with a new ray between leaves.
 struct TravState {
+#if !HPT_RAY_IN_SMEM
   Ray ray;
+#endif
   float t_entry;         // current entry distance
   int32_t node;          // node to descend from, -1 = finished
   int32_t steps;
@@ -125,8 +134,31 @@ struct TravCold {
   int32_t ties;       // bits 0-2: axes with a zero direction component;
                       // 3-5: axes on which a descent met such a plane;
                       // 6-8: axes whose planes this walk passes on the right
+#if HPT_RAY_IN_SMEM
+  Ray ray;
+#endif
 };
-static_assert(sizeof(TravCold) == 52, "odd word stride in shared memory");
+static_assert(sizeof(TravCold) == (HPT_RAY_IN_SMEM ? 76 : 52), "odd word stride in shared memory");
+
+// The walking ray of a lane.
+HPT_HD Ray& ray_of(TravState& st, TravCold& tc) {
+#if HPT_RAY_IN_SMEM
+  (void)st;
+  return tc.ray;
+#else
+  (void)tc;
+  return st.ray;
+#endif
+}
+HPT_HD const Ray& ray_of(const TravState& st, const TravCold& tc) {
+#if HPT_RAY_IN_SMEM
+  (void)st;
+  return tc.ray;
+#else
+  (void)tc;
+  return st.ray;
+#endif
+}
 
 // A ray with a zero direction component whose coordinate equals a node's
 // split on that axis lies in the plane between the two children, and a
@@ -178,7 +210,7 @@ struct TravCount {
 template <class Sc>
 HPT_HD void trav_init(const Sc& s, const Ray& r, TravState& st, TravCold& tc,
                       int start_node = -1) {
-  st.ray = r;
+  ray_of(st, tc) = r;
   st.best.rec = -1;
   st.best.tri = -1;
   st.best.t = 0.f;
@@ -285,7 +317,7 @@ HPT_HD bool trav_leaf(const Sc& s, TravState& st, TravCold& tc, const uint2* sme
                       int n_smem, DevErr* err, TravCount& cnt) {
   if (st.node < 0) return true;
   HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
-  const Ray& r = st.ray;
+  const Ray& r = ray_of(st, tc);
   // Entry point p = o + t_entry * d (kernel.cl:291 style, no FMA).
   const float px = rn_add(r.o.x, rn_mul(st.t_entry, r.d.x));
   const float py = rn_add(r.o.y, rn_mul(st.t_entry, r.d.y));
@@ -414,6 +446,30 @@ HPT_HD bool trav_leaf(const Sc& s, TravState& st, TravCold& tc, const uint2* sme
   return false;
 }
 
+// Leaf exit of the step-at-a-time walk, once every triangle of the current
+// leaf was tested: stop once the rest of the ray starts beyond the best hit
+// (+ slack), else follow the exit rope. A leaf without an exit face has
+// t_exit = +inf and stops here. Returns true when the ray is finished.
+template <class Sc>
+HPT_HD bool trav_exit(const Sc& s, TravState& st, TravCold& tc, DevErr* err) {
+  st.phase = kStepDescend;
+  const int rope = tc.rope;
+  if (!(tc.t_exit < tc.t_end) || rope < 0 ||
+      (st.best.rec >= 0 &&
+       tc.t_exit > rn_add(st.best.t, rn_add(rn_mul(st.best.t, 1e-4f), tc.slack))))
+    return trav_finish(st, tc);
+  if (st.steps > s.max_steps) {
+    hpt_atomic_or(&err->flags, 1u);
+    st.node = -1;
+    return true;
+  }
+  HPT_DCHECK(err, rope < s.num_nodes, 105, rope, { st.node = -1; return true; });
+  st.node = rope;
+  st.t_entry = fmaxf(st.t_entry, tc.t_exit);
+  return false;
+}
+
+
 // --- Step-at-a-time traversal ----------------------------------------------
 // The same walk as trav_leaf, cut into units of similar cost: one descent
 // step, the set-up of a newly reached leaf, one triangle test, or the exit
@@ -432,11 +488,13 @@ HPT_HD bool trav_leaf(const Sc& s, TravState& st, TravCold& tc, const uint2* sme
 // Returns true when the ray is finished.
 // kSmem: nodes below n_smem are read from the shared-memory prefix (false:
 // every node from global memory, and smem / n_smem are ignored).
-template <bool kUV = false, bool kSmem = true, class Sc = DevScene>
+// kTests = false: the caller only calls it in the descent phase (its
+// triangle tests run elsewhere), so the test unit is left out.
+template <bool kUV = false, bool kSmem = true, class Sc = DevScene, bool kTests = true>
 HPT_HD bool trav_step(const Sc& s, TravState& st, TravCold& tc, const uint2* smem,
                       int n_smem, DevErr* err, TravCount& cnt) {
   if (st.node < 0) return true;
-  const Ray& r = st.ray;
+  const Ray& r = ray_of(st, tc);
   if (st.phase == kStepDescend) {
     HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
     const uint2 nd = fetch_node(s, smem, kSmem ? n_smem : 0, st.node);
@@ -508,6 +566,7 @@ HPT_HD bool trav_step(const Sc& s, TravState& st, TravCold& tc, const uint2* sme
     st.phase = kStepTest;
     return false;
   }
+  if constexpr (!kTests) return false;
   if (st.k < st.end) {
     // One triangle test (the body of trav_leaf's triangle loop).
     const int j = st.k++;
@@ -563,24 +622,7 @@ HPT_HD bool trav_step(const Sc& s, TravState& st, TravCold& tc, const uint2* sme
     if (st.k < st.end) return false;
     // The leaf's last test falls through to its exit.
   }
-  // Leaf exit: stop once the rest of the ray starts beyond the best hit
-  // (+ slack), else follow the exit rope. A leaf without an exit face has
-  // t_exit = +inf and stops here.
-  st.phase = kStepDescend;
-  const int rope = tc.rope;
-  if (!(tc.t_exit < tc.t_end) || rope < 0 ||
-      (st.best.rec >= 0 &&
-       tc.t_exit > rn_add(st.best.t, rn_add(rn_mul(st.best.t, 1e-4f), tc.slack))))
-    return trav_finish(st, tc);
-  if (st.steps > s.max_steps) {
-    hpt_atomic_or(&err->flags, 1u);
-    st.node = -1;
-    return true;
-  }
-  HPT_DCHECK(err, rope < s.num_nodes, 105, rope, { st.node = -1; return true; });
-  st.node = rope;
-  st.t_entry = fmaxf(st.t_entry, tc.t_exit);
-  return false;
+  return trav_exit(s, st, tc, err);
 }
 
 }  // namespace hpt
