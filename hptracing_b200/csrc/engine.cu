@@ -345,11 +345,6 @@ __device__ __forceinline__ bool coop_tests(const SceneOf& scene_of, int slot, bo
   const int o_excl = __shfl_sync(kFull, excl, owner);
   const int o_mb = __shfl_sync(kFull, st.mb_id[0], owner);
   const int o_slot = __shfl_sync(kFull, slot, owner);
-#if HPT_RAY_IN_SMEM
-  // The owner's TravCold sits (owner - lane) entries away in the block's
-  // per-lane array.
-  const Ray r = (&tc)[owner - lane].ray;
-#else
   Ray r;
   r.o.x = __shfl_sync(kFull, st.ray.o.x, owner);
   r.o.y = __shfl_sync(kFull, st.ray.o.y, owner);
@@ -357,7 +352,6 @@ __device__ __forceinline__ bool coop_tests(const SceneOf& scene_of, int slot, bo
   r.d.x = __shfl_sync(kFull, st.ray.d.x, owner);
   r.d.y = __shfl_sync(kFull, st.ray.d.y, owner);
   r.d.z = __shfl_sync(kFull, st.ray.d.z, owner);
-#endif
   int id = -1;
   uint32_t key = ~0u;  // t's bits for a hit (t > 0: ordered like t), else the maximum
   if (valid) {
@@ -420,7 +414,7 @@ __device__ __forceinline__ bool coop_tests(const SceneOf& scene_of, int slot, bo
         const auto& s = scene_of(slot);
         if (tc.pierced < 0) {
           const float4* L = reinterpret_cast<const float4*>(s.leaves + tc.leaf);
-          tc.pierced = ref_box_test(ray_of(st, tc), ldg(L), ldg(L + 1)) ? 1 : 0;
+          tc.pierced = ref_box_test(st.ray, ldg(L), ldg(L + 1)) ? 1 : 0;
         }
         if (tc.pierced) {
           st.best.rec = jb;
@@ -510,8 +504,7 @@ __device__ __forceinline__ void prim_finish(const EngineParams& P, int slot, int
     HPT_DCHECK(&P.ctrl->err, k < job_rays(J), 203, k, k = -1);
     if (k >= 0) {
       float4* dst = reinterpret_cast<float4*>(J.prim) + 2 * (size_t)k;
-      const f3 d = ray_of(st, tc).d;
-      dst[0] = make_float4(d.x, d.y, d.z, __int_as_float((int)ray));
+      dst[0] = make_float4(st.ray.d.x, st.ray.d.y, st.ray.d.z, __int_as_float((int)ray));
       dst[1] = make_float4(__int_as_float(st.best.tri), st.best.t, __int_as_float(tc.best_node),
                            0.f);
     }

@@ -86,19 +86,10 @@ constexpr int kMailbox = HPT_MAILBOX;
 constexpr int32_t kStepDescend = 0;
 constexpr int32_t kStepTest = 1;
 
-// Where a walking ray's origin and direction live: in TravState (registers)
-// or, built with -DHPT_RAY_IN_SMEM=1, in TravCold (shared memory in the
-// kernels), which frees six registers per lane.
-#ifndef HPT_RAY_IN_SMEM
-#define HPT_RAY_IN_SMEM 0
-#endif
-
 // Traversal state of one ray that most units touch; lives in registers so
 // a lane can be refilled with a new ray between leaves.
 struct TravState {
-#if !HPT_RAY_IN_SMEM
   Ray ray;
-#endif
   float t_entry;         // current entry distance
   int32_t node;          // node to descend from, -1 = finished
   int32_t steps;
@@ -134,31 +125,8 @@ struct TravCold {
   int32_t ties;       // bits 0-2: axes with a zero direction component;
                       // 3-5: axes on which a descent met such a plane;
                       // 6-8: axes whose planes this walk passes on the right
-#if HPT_RAY_IN_SMEM
-  Ray ray;
-#endif
 };
-static_assert(sizeof(TravCold) == (HPT_RAY_IN_SMEM ? 76 : 52), "odd word stride in shared memory");
-
-// The walking ray of a lane.
-HPT_HD Ray& ray_of(TravState& st, TravCold& tc) {
-#if HPT_RAY_IN_SMEM
-  (void)st;
-  return tc.ray;
-#else
-  (void)tc;
-  return st.ray;
-#endif
-}
-HPT_HD const Ray& ray_of(const TravState& st, const TravCold& tc) {
-#if HPT_RAY_IN_SMEM
-  (void)st;
-  return tc.ray;
-#else
-  (void)tc;
-  return st.ray;
-#endif
-}
+static_assert(sizeof(TravCold) == 52, "odd word stride in shared memory");
 
 // A ray with a zero direction component whose coordinate equals a node's
 // split on that axis lies in the plane between the two children, and a
@@ -210,7 +178,7 @@ struct TravCount {
 template <class Sc>
 HPT_HD void trav_init(const Sc& s, const Ray& r, TravState& st, TravCold& tc,
                       int start_node = -1) {
-  ray_of(st, tc) = r;
+  st.ray = r;
   st.best.rec = -1;
   st.best.tri = -1;
   st.best.t = 0.f;
@@ -317,7 +285,7 @@ HPT_HD bool trav_leaf(const Sc& s, TravState& st, TravCold& tc, const uint2* sme
                       int n_smem, DevErr* err, TravCount& cnt) {
   if (st.node < 0) return true;
   HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
-  const Ray& r = ray_of(st, tc);
+  const Ray& r = st.ray;
   // Entry point p = o + t_entry * d (kernel.cl:291 style, no FMA).
   const float px = rn_add(r.o.x, rn_mul(st.t_entry, r.d.x));
   const float py = rn_add(r.o.y, rn_mul(st.t_entry, r.d.y));
@@ -494,7 +462,7 @@ template <bool kUV = false, bool kSmem = true, class Sc = DevScene, bool kTests 
 HPT_HD bool trav_step(const Sc& s, TravState& st, TravCold& tc, const uint2* smem,
                       int n_smem, DevErr* err, TravCount& cnt) {
   if (st.node < 0) return true;
-  const Ray& r = ray_of(st, tc);
+  const Ray& r = st.ray;
   if (st.phase == kStepDescend) {
     HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
     const uint2 nd = fetch_node(s, smem, kSmem ? n_smem : 0, st.node);
