@@ -809,7 +809,7 @@ def run_compact(args):
             "unit": "GB/s", "n": n, "survivors": total, "exact": exact,
             "ms_per_call": ms, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True,
-            "roofline": {"bound": "hbm", "kernel": "k_compact_count+scan+scatter",
+            "roofline": {"bound": "hbm", "kernel": "k_compact_count+k_compact_scatter",
                          "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": alg / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_call": alg},
