@@ -272,6 +272,7 @@ constexpr int kTravStepSmem = 2;  // trav_step with the shared-memory node prefi
 #ifndef HPT_COOP_TEST_SIXTHS
 #define HPT_COOP_TEST_SIXTHS 1
 #endif
+
 // k_primary tests one reference per testing lane a round unless built with
 // -DHPT_COOP_PRIMARY=1: camera rays are coherent, neighbouring lanes test
 // the same triangles and share their loads, and the terrain frame's
@@ -318,10 +319,9 @@ struct JobScene {
 // scene_of(slot) gives (a lane may test for a ray of another job, so it
 // reads that ray's scene). Returns true when this lane's ray finished (its
 // leaf's last reference was tested and the exit ended it).
-template <class SceneOf>
+template <class SceneOf, class Cnt>
 __device__ __forceinline__ bool coop_tests(const SceneOf& scene_of, int slot, bool testing,
-                                           TravState& st, TravCold& tc, DevErr* err,
-                                           TravCount& cnt) {
+                                           TravState& st, TravCold& tc, DevErr* err, Cnt& cnt) {
   const int lane = threadIdx.x & 31;
   const int rem = testing ? st.end - st.k : 0;
   // This lane's references take slots [excl, incl) of the round.
@@ -373,8 +373,8 @@ __device__ __forceinline__ bool coop_tests(const SceneOf& scene_of, int slot, bo
   // equal to the one before it in its ray's sequence is a mailbox repeat.
   const int up = __shfl_up_sync(kFull, id, 1);
   if (valid) {
-    if (id == (lane == o_excl ? o_mb : up)) ++cnt.repeats;
-    else ++cnt.tris;
+    if (id == (lane == o_excl ? o_mb : up)) count_repeat(cnt);
+    else count_test(cnt);
   }
   // Segmented minimum of t: the first slot of each ray's range ends with
   // its range's minimum. Bit s of `starts`: slot s begins a range.
@@ -439,6 +439,10 @@ __device__ __forceinline__ bool vote_units(const SceneOf& scene_of, int slot, bo
                                            TravState& st, TravCold& tc, const uint2* snodes,
                                            int n_smem, DevErr* err, TravCount& cnt, int units) {
   bool finished = false;
+  // The cooperative loop's work counts stay in one register and are added
+  // to the shared-memory counters at most 128 rounds apart and on return
+  // (a shared-memory update per unit measured 1-2 % slower).
+  PackedCount ucnt{0};
   for (int u = 0; u < units; ++u) {
     const bool go = live && !finished;
     const unsigned lm = __ballot_sync(kFull, go);
@@ -447,15 +451,16 @@ __device__ __forceinline__ bool vote_units(const SceneOf& scene_of, int slot, bo
     const unsigned tm = __ballot_sync(kFull, testing);
 #if HPT_COOP_TESTS
     if constexpr (kCoop) {
+      using SceneT = std::decay_t<decltype(scene_of(slot))>;
       // Every round moves a lane on: a test round needs a testing lane
       // (whatever the threshold), else the descending lanes run.
       if (tm != 0 && 6 * __popc(tm) >= HPT_COOP_TEST_SIXTHS * __popc(lm)) {
-        if (coop_tests(scene_of, slot, testing, st, tc, err, cnt)) finished = true;
+        if (coop_tests(scene_of, slot, testing, st, tc, err, ucnt)) finished = true;
       } else if (go && !testing) {
-        finished = trav_step<false, kMode == kTravStepSmem,
-                             std::decay_t<decltype(scene_of(slot))>, false>(
-            scene_of(slot), st, tc, snodes, n_smem, err, cnt);
+        finished = trav_step<false, kMode == kTravStepSmem, SceneT, false>(
+            scene_of(slot), st, tc, snodes, n_smem, err, ucnt);
       }
+      if ((u & 127) == 127) count_flush(ucnt, cnt);
       continue;
     }
 #endif
@@ -464,6 +469,7 @@ __device__ __forceinline__ bool vote_units(const SceneOf& scene_of, int slot, bo
       finished = trav_step<false, kMode == kTravStepSmem>(scene_of(slot), st, tc, snodes, n_smem,
                                                           err, cnt);
   }
+  count_flush(ucnt, cnt);
   return finished;
 }
 #endif

@@ -172,6 +172,28 @@ struct TravCount {
   uint32_t nodes, leaves, tris, repeats;
 };
 
+// The work counters of a run of traversal units in one register: four
+// 8-bit fields (nodes, leaves, triangle tests, mailbox repeats), added into
+// a TravCount by count_flush before any field can pass 255.
+struct PackedCount {
+  uint32_t v;
+};
+HPT_HD void count_node(TravCount& c) { ++c.nodes; }
+HPT_HD void count_leaf(TravCount& c) { ++c.leaves; }
+HPT_HD void count_test(TravCount& c) { ++c.tris; }
+HPT_HD void count_repeat(TravCount& c) { ++c.repeats; }
+HPT_HD void count_node(PackedCount& c) { c.v += 1u; }
+HPT_HD void count_leaf(PackedCount& c) { c.v += 1u << 8; }
+HPT_HD void count_test(PackedCount& c) { c.v += 1u << 16; }
+HPT_HD void count_repeat(PackedCount& c) { c.v += 1u << 24; }
+HPT_HD void count_flush(PackedCount& p, TravCount& c) {
+  c.nodes += p.v & 255u;
+  c.leaves += (p.v >> 8) & 255u;
+  c.tris += (p.v >> 16) & 255u;
+  c.repeats += p.v >> 24;
+  p.v = 0;
+}
+
 // Starts a query. start_node (>= 0) names a leaf node the origin is
 // expected to lie in (the leaf of the previous hit): if its box contains the
 // origin the walk starts there instead of descending from the root.
@@ -437,6 +459,57 @@ HPT_HD bool trav_exit(const Sc& s, TravState& st, TravCold& tc, DevErr* err) {
   return false;
 }
 
+// Leaf set-up of the step-at-a-time walk for the leaf record st.k, reached
+// at node st.node: exit distance and face, triangle range; the walk then
+// tests the leaf's triangles (phase kStepTest). Returns true when the ray is
+// finished (a failed self-check).
+template <class Sc, class Cnt>
+HPT_HD bool trav_setup(const Sc& s, TravState& st, TravCold& tc, DevErr* err, Cnt& cnt) {
+  const Ray& r = st.ray;
+  const int leaf = st.k;
+  const float4* L = reinterpret_cast<const float4*>(s.leaves + leaf);
+  // The six ropes are read with the box (independent loads) so that the
+  // exit needs no dependent load of its own.
+  const float4 L0 = ldg(L), L1 = ldg(L + 1);
+  const int4 R03 = ldg(reinterpret_cast<const int4*>(L + 2));
+  const int2 R45 = ldg(reinterpret_cast<const int2*>(L + 3));
+  float t_exit = as_float(0x7f800000);
+  int face = -1;
+  {
+    const float d[3] = {r.d.x, r.d.y, r.d.z};
+    const float o[3] = {r.o.x, r.o.y, r.o.z};
+    const float iv[3] = {tc.inv_d.x, tc.inv_d.y, tc.inv_d.z};
+    const float lo[3] = {L0.x, L0.y, L0.z};
+    const float hi[3] = {L1.x, L1.y, L1.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (d[a] != 0.f) {
+        const float tf = rn_mul(rn_sub(d[a] > 0.f ? hi[a] : lo[a], o[a]), iv[a]);
+        if (tf < t_exit) {
+          t_exit = tf;
+          face = 2 * a + (d[a] > 0.f ? 1 : 0);
+        }
+      }
+    }
+  }
+  const int begin = as_int(L0.w), count = as_int(L1.w);
+  count_leaf(cnt);
+  HPT_DCHECK(err, begin >= 0 && count >= 0 && (long long)begin + count <= s.num_leaf_tris, 103,
+             begin, { st.node = -1; return true; });
+  // trav_leaf adds the leaf's cost when it leaves it; every comparison with
+  // max_steps comes later in both orders, so adding it here is equivalent.
+  st.steps += 1 + count;
+  st.k = begin;
+  st.end = begin + count;
+  tc.leaf = leaf;
+  tc.leaf_node = st.node;
+  tc.rope = face == 0 ? R03.x : face == 1 ? R03.y : face == 2 ? R03.z
+          : face == 3 ? R03.w : face == 4 ? R45.x : face == 5 ? R45.y : -1;
+  tc.t_exit = t_exit;
+  tc.pierced = -1;
+  st.phase = kStepTest;
+  return false;
+}
 
 // --- Step-at-a-time traversal ----------------------------------------------
 // The same walk as trav_leaf, cut into units of similar cost: one descent
@@ -458,9 +531,10 @@ HPT_HD bool trav_exit(const Sc& s, TravState& st, TravCold& tc, DevErr* err) {
 // every node from global memory, and smem / n_smem are ignored).
 // kTests = false: the caller only calls it in the descent phase (its
 // triangle tests run elsewhere), so the test unit is left out.
-template <bool kUV = false, bool kSmem = true, class Sc = DevScene, bool kTests = true>
+template <bool kUV = false, bool kSmem = true, class Sc = DevScene, bool kTests = true,
+          class Cnt = TravCount>
 HPT_HD bool trav_step(const Sc& s, TravState& st, TravCold& tc, const uint2* smem,
-                      int n_smem, DevErr* err, TravCount& cnt) {
+                      int n_smem, DevErr* err, Cnt& cnt) {
   if (st.node < 0) return true;
   const Ray& r = st.ray;
   if (st.phase == kStepDescend) {
@@ -479,7 +553,7 @@ HPT_HD bool trav_step(const Sc& s, TravState& st, TravCold& tc, const uint2* sme
       HPT_DCHECK(err, (int)(nd.x & kIndexMask) + 1 < s.num_nodes, 106, nd.x & kIndexMask,
                  { st.node = -1; return true; });
       st.node = (int)(nd.x & kIndexMask) + (right ? 1 : 0);
-      ++cnt.nodes;
+      count_node(cnt);
       if (++st.steps > s.max_steps) {
         hpt_atomic_or(&err->flags, 1u);
         st.node = -1;
@@ -487,52 +561,10 @@ HPT_HD bool trav_step(const Sc& s, TravState& st, TravCold& tc, const uint2* sme
       }
       return false;
     }
-    // Leaf set-up: exit distance and face, triangle range.
     HPT_DCHECK(err, (int)(nd.x & kIndexMask) < s.num_leaves, 102, nd.x & kIndexMask,
                { st.node = -1; return true; });
-    const int leaf = (int)(nd.x & kIndexMask);
-    const float4* L = reinterpret_cast<const float4*>(s.leaves + leaf);
-    // The six ropes are read with the box (independent loads) so that the
-    // exit needs no dependent load of its own.
-    const float4 L0 = ldg(L), L1 = ldg(L + 1);
-    const int4 R03 = ldg(reinterpret_cast<const int4*>(L + 2));
-    const int2 R45 = ldg(reinterpret_cast<const int2*>(L + 3));
-    float t_exit = as_float(0x7f800000);
-    int face = -1;
-    {
-      const float d[3] = {r.d.x, r.d.y, r.d.z};
-      const float o[3] = {r.o.x, r.o.y, r.o.z};
-      const float iv[3] = {tc.inv_d.x, tc.inv_d.y, tc.inv_d.z};
-      const float lo[3] = {L0.x, L0.y, L0.z};
-      const float hi[3] = {L1.x, L1.y, L1.z};
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        if (d[a] != 0.f) {
-          const float tf = rn_mul(rn_sub(d[a] > 0.f ? hi[a] : lo[a], o[a]), iv[a]);
-          if (tf < t_exit) {
-            t_exit = tf;
-            face = 2 * a + (d[a] > 0.f ? 1 : 0);
-          }
-        }
-      }
-    }
-    const int begin = as_int(L0.w), count = as_int(L1.w);
-    ++cnt.leaves;
-    HPT_DCHECK(err, begin >= 0 && count >= 0 && (long long)begin + count <= s.num_leaf_tris, 103,
-               begin, { st.node = -1; return true; });
-    // trav_leaf adds the leaf's cost when it leaves it; every comparison with
-    // max_steps comes later in both orders, so adding it here is equivalent.
-    st.steps += 1 + count;
-    st.k = begin;
-    st.end = begin + count;
-    tc.leaf = leaf;
-    tc.leaf_node = st.node;
-    tc.rope = face == 0 ? R03.x : face == 1 ? R03.y : face == 2 ? R03.z
-            : face == 3 ? R03.w : face == 4 ? R45.x : face == 5 ? R45.y : -1;
-    tc.t_exit = t_exit;
-    tc.pierced = -1;
-    st.phase = kStepTest;
-    return false;
+    st.k = (int)(nd.x & kIndexMask);
+    return trav_setup(s, st, tc, err, cnt);
   }
   if constexpr (!kTests) return false;
   if (st.k < st.end) {
@@ -548,12 +580,12 @@ HPT_HD bool trav_step(const Sc& s, TravState& st, TravCold& tc, const uint2* sme
     for (int m = 0; m < kMailbox; ++m)
       if (st.mb_id[m] == id) slot = m;
     if (slot >= 0) {
-      ++cnt.repeats;
+      count_repeat(cnt);
 #pragma unroll
       for (int m = 0; m < kMailbox; ++m)
         if (m == slot) t = st.mb_t[m];
     } else {
-      ++cnt.tris;
+      count_test(cnt);
       const float4* rec = recs + 3 * (size_t)id;
       const float4 A = ldg(rec), E1 = ldg(rec + 1), E2 = ldg(rec + 2);
       if (!mt_test(r, A, E1, E2, t, u, v)) t = -1.f;
