@@ -208,7 +208,9 @@ def make_camera(view_p, top_dir, right_dir, width, height):
 
 
 def make_params(sample_x, sample_y, supersample_x=1, supersample_y=1, background=(0, 0, 0),
-                sample=10, depth=6, disable_diffuse=0, brightness=1.0, seed=0):
+                sample=10, depth=6, disable_diffuse=0, brightness=1.0, seed=0, first_sample=0):
+    """hpt_render_params. first_sample: the frame's index of this render's
+    first sample (a frame's spp split over several renders)."""
     p = RenderParams()
     p.sample_x, p.sample_y = int(sample_x), int(sample_y)
     p.supersample_x, p.supersample_y = int(supersample_x), int(supersample_y)
@@ -217,6 +219,7 @@ def make_params(sample_x, sample_y, supersample_x=1, supersample_y=1, background
     p.disable_diffuse = int(disable_diffuse)
     p.brightness = float(brightness)
     p.seed = int(seed)
+    p.first_sample = int(first_sample)
     return p
 
 

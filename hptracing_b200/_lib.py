@@ -79,7 +79,8 @@ class Camera(C.Structure):
 class RenderParams(C.Structure):
     _fields_ = [("sample_x", i32), ("sample_y", i32), ("supersample_x", i32),
                 ("supersample_y", i32), ("background", f32 * 3), ("sample", i32),
-                ("depth", i32), ("disable_diffuse", i32), ("brightness", f32), ("seed", u64)]
+                ("depth", i32), ("disable_diffuse", i32), ("brightness", f32), ("seed", u64),
+                ("first_sample", i32)]
 
 
 class RenderStats(C.Structure):

@@ -112,6 +112,7 @@ struct DevJob {
   int32_t vr_x_shift;       // int(right.x) * supersample_x
   float bg[3];
   int32_t spp, depth, disable_diffuse;
+  int32_t first_sample;     // the frame's index of this job's sample 0 (RNG key)
   uint64_t seed;
   unsigned long long* accum;  // 3 x fixed-point u64 per ray
   uint32_t* flags;          // per ray: NaN / +inf / -inf markers (4 bits per channel)

@@ -29,6 +29,7 @@
 // bounce) and radiance is summed in 2^-32 fixed point, so a job's image does
 // not depend on how its paths are scheduled, batched or interleaved.
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -739,7 +740,11 @@ __global__ void __launch_bounds__(BS, MINB) k_shade(EngineParams P) {
       HPT_DCHECK(&c->err, !ok || (ray >= 0 && ray < job_rays(P.jobs[slot])), 215, ray, ok = false);
       if (ok) {
         const DevJob& J = P.jobs[slot];
-        uint64_t seed = path_seed(J.seed, (uint32_t)ray, (uint32_t)sample, (uint32_t)bounce);
+        // The frame's sample index keys the random stream, so a render of
+        // samples [first_sample, first_sample + spp) traces the same paths
+        // as those samples of one whole-frame render.
+        uint64_t seed = path_seed(J.seed, (uint32_t)ray, (uint32_t)(J.first_sample + sample),
+                                  (uint32_t)bounce);
         const Ray r{o, d};
         const ShadeOut so = shade_hit(J.scene, r, strength, tri, t, J.disable_diffuse, seed,
                                       &c->err);
@@ -1160,6 +1165,8 @@ hpt_status check_render_params(const hpt_camera* cam, const hpt_render_params* p
   const int64_t rays = (int64_t)p->sample_x * p->supersample_x * p->sample_y * p->supersample_y;
   if (rays > (1ll << 30)) return fail(HPT_ERR_INVALID_ARGUMENT, "too many rays per frame");
   if (p->sample >= (1 << 24)) return fail(HPT_ERR_INVALID_ARGUMENT, "sample must be < 2^24");
+  if (p->first_sample < 0 || p->first_sample > INT32_MAX - p->sample)
+    return fail(HPT_ERR_INVALID_ARGUMENT, "first_sample must be >= 0 and first_sample + sample < 2^31");
   if (p->depth > 255) return fail(HPT_ERR_INVALID_ARGUMENT, "depth must be <= 255");
   if (cam->height < 0 && p->supersample_x != p->supersample_y)
     return fail(HPT_ERR_INVALID_ARGUMENT,
@@ -1439,6 +1446,7 @@ DevJob Engine::make_job(const JobSpec& js, const JobBuffers& b) const {
   j.spp = p.sample;
   j.depth = p.depth;
   j.disable_diffuse = p.disable_diffuse;
+  j.first_sample = p.first_sample;
   j.seed = p.seed;
   j.accum = b.accum;
   j.flags = b.flags;

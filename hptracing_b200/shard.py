@@ -55,3 +55,75 @@ def allreduce_sum(x, world, device="cuda"):
     """Sum of x over the ranks."""
     import torch.distributed as dist
     return _reduce(x, dist.ReduceOp.SUM if world > 1 else None, world, device)
+
+
+# --- One frame's samples over the ranks ------------------------------------
+# The random stream of a path is keyed by (ray, the frame's sample index,
+# bounce), and a render of samples [f, f + n) of a frame (first_sample = f)
+# traces exactly the paths of those samples of one whole-frame render. So a
+# frame can be split by samples over N GPUs with one exchange step: the sum
+# of the per-ray radiance accumulators (w*h*ss^2 * 3 floats), after which
+# any rank resolves the image.
+
+def spp_slices(spp, world):
+    """Samples [0, spp) in `world` contiguous slices, the first spp % world
+    ranks taking one more: a list of (first_sample, count) per rank (count 0
+    for a rank with nothing to render)."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    if spp < 1:
+        raise ValueError("spp must be >= 1")
+    base, extra = divmod(int(spp), world)
+    out, first = [], 0
+    for r in range(world):
+        n = base + (1 if r < extra else 0)
+        out.append((first, n))
+        first += n
+    return out
+
+
+def split_spp_accum(render_slice, spp, rays, rank, world, device="cuda"):
+    """This rank's slice of a frame's samples, summed over the ranks.
+
+    render_slice(first, count) renders samples [first, first + count) and
+    returns their (rays, 3) float32 accumulator; it is not called for an
+    empty slice. The accumulators are added with one all-reduce over the
+    process group (NCCL between GPUs, gloo on CPU); every rank returns the
+    frame's (rays, 3) sum."""
+    import numpy as np
+    first, count = spp_slices(spp, world)[rank]
+    acc = (np.asarray(render_slice(first, count), np.float32).reshape(rays, 3)
+           if count > 0 else np.zeros((rays, 3), np.float32))
+    if world == 1:
+        return acc
+    import torch
+    import torch.distributed as dist
+    t = torch.from_numpy(np.ascontiguousarray(acc)).to(device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return t.cpu().numpy()
+
+
+def render_split_spp(scene, camera, params, rank, world, device="cuda"):
+    """One frame (hpt_render_params `params`) with its samples split over the
+    ranks: each rank renders its slice on its own GPU (`scene` lives there),
+    the accumulators are summed with one all-reduce and the image is resolved
+    from the sum. Returns (rgba, accum) of the whole frame on every rank.
+    The sum equals one render of all the samples up to float32 rounding of
+    the per-ray accumulators (the renders add radiance in 2^-32 fixed point
+    and hand out float32 sums)."""
+    import ctypes
+
+    import hptracing_b200 as H
+    rays = (params.sample_x * params.supersample_x * params.sample_y * params.supersample_y)
+
+    def render_slice(first, count):
+        p = H.RenderParams()
+        ctypes.memmove(ctypes.byref(p), ctypes.byref(params), ctypes.sizeof(p))
+        p.sample = count
+        p.first_sample = params.first_sample + first
+        return scene.render(camera, p, want_accum=True)[1]
+
+    acc = split_spp_accum(render_slice, params.sample, rays, rank, world, device)
+    rgba = H.resolve(acc, params.sample_x, params.sample_y, params.supersample_x,
+                     params.supersample_y, params.sample, params.brightness)
+    return rgba, acc

@@ -233,6 +233,12 @@ typedef struct hpt_render_params {
   int32_t disable_diffuse;
   float brightness;
   uint64_t seed;           /* counter-based RNG key                      */
+  int32_t first_sample;    /* index of this render's first sample, >= 0 */
+                           /* (0 for a whole frame). Renders of samples  */
+                           /* [f, f + sample) of one frame trace the     */
+                           /* paths one render of all its samples would; */
+                           /* their accumulators add up to its (spp     */
+                           /* split over GPUs, one reduction).           */
 } hpt_render_params;
 
 typedef struct hpt_render_stats {

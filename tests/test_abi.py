@@ -164,3 +164,42 @@ def test_loader_keeps_per_texture_sizes(built, tmp_path):
     assert len(m4.texture_data) == 2 * 4 * 4 * 4
     with pytest.raises(H.HptError):
         H.Mesh.load_obj(path, str(tmp_path) + "/", texture_size=-1)
+
+
+# Every struct the ctypes binding mirrors, against the C compiler's layout of
+# include/hpt.h: size and the offset of each field.
+_MIRRORS = {
+    "hpt_ref_node": _lib.RefNode, "hpt_ref_material": _lib.RefMaterial,
+    "hpt_mesh_arrays": _lib.MeshArrays, "hpt_gen_params": _lib.GenParams,
+    "hpt_scene_desc": _lib.SceneDesc, "hpt_scene_info": _lib.SceneInfo,
+    "hpt_camera": _lib.Camera, "hpt_render_params": _lib.RenderParams,
+    "hpt_render_stats": _lib.RenderStats, "hpt_tuning": _lib.Tuning,
+    "hpt_server_config": _lib.ServerConfig, "hpt_request_info": _lib.RequestInfo,
+}
+
+
+def test_ctypes_mirrors_match_the_c_layout(tmp_path):
+    gcc = __import__("shutil").which("gcc")
+    if not gcc:
+        pytest.skip("no C compiler")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "hpt.h"', 'int main(void) {']
+    for cname, cls in _MIRRORS.items():
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
+        for fname, _ in cls._fields_:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));'
+                         % (cname, fname, cname, fname))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run([gcc, "-I", inc, str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                               text=True).stdout.splitlines():
+        cname, field, value = line.split()
+        got[(cname, field)] = int(value)
+    for cname, cls in _MIRRORS.items():
+        assert got[(cname, "size")] == C.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)

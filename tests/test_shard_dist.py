@@ -70,3 +70,74 @@ def test_two_gloo_ranks_agree_on_the_table_and_reduce():
     assert m0 == m1 == max(loads)
     assert s0 == s1 == sum(costs)
     assert c0 == c1 == len(costs)
+
+
+def test_spp_slices_partition_the_samples():
+    for spp in (1, 2, 7, 64, 257):
+        for world in (1, 2, 3, 4, 8):
+            sl = shard.spp_slices(spp, world)
+            assert len(sl) == world
+            # contiguous, in rank order, covering [0, spp) exactly
+            assert sl[0][0] == 0
+            for (f0, n0), (f1, _) in zip(sl, sl[1:]):
+                assert f1 == f0 + n0
+            assert sum(n for _, n in sl) == spp
+            assert max(n for _, n in sl) - min(n for _, n in sl) <= 1
+    with pytest.raises(ValueError):
+        shard.spp_slices(4, 0)
+    with pytest.raises(ValueError):
+        shard.spp_slices(0, 2)
+
+
+RAYS = 40
+SPP = 7
+
+
+def _fake_slice(first, count):
+    """Stand-in for a render of samples [first, first + count): per ray and
+    sample an integer-valued radiance, so float sums are exact in any order."""
+    import numpy as np
+    acc = np.zeros((RAYS, 3), np.float32)
+    for s in range(first, first + count):
+        acc += (np.arange(RAYS * 3, dtype=np.float32).reshape(RAYS, 3) * (s + 1)) % 97
+    return acc
+
+
+def _split_rank_main(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        calls = []
+
+        def render(first, count):
+            calls.append((first, count))
+            return _fake_slice(first, count)
+
+        acc = shard.split_spp_accum(render, SPP, RAYS, rank, world, device="cpu")
+        out.put((rank, calls, acc.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_split_one_frames_samples():
+    """Each rank renders only its slice of the samples; after the one
+    all-reduce both hold the accumulator of all the samples."""
+    import numpy as np
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_split_rank_main, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted((r, c, a) for r, c, a in (out.get(timeout=120) for _ in procs))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (r0, c0, a0), (r1, c1, a1) = res
+    assert c0 == [(0, 4)] and c1 == [(4, 3)]
+    whole = _fake_slice(0, SPP)
+    assert np.array_equal(np.asarray(a0, np.float32), whole)
+    assert np.array_equal(np.asarray(a1, np.float32), whole)
