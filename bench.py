@@ -68,9 +68,10 @@ def parse():
     ap.add_argument("--mode", default="frame", choices=["frame", "batch", "serve", "compact"])
     ap.add_argument("--compact-n", type=int, default=1 << 25,
                     help="compact: number of flags")
-    ap.add_argument("--scene", default="spheres", choices=["spheres", "terrain"],
-                    help="frame: the 61k-triangle spheres frame (headline) or the "
-                         "2.4M-triangle terrain at 1920x1080, 256 spp")
+    ap.add_argument("--scene", default="spheres", choices=["spheres", "terrain", "room"],
+                    help="frame: the 61k-triangle spheres frame (headline), the "
+                         "2.4M-triangle terrain at 1920x1080, 256 spp, or the 38-triangle "
+                         "box room at 256x256, 16 spp, depth 5")
     ap.add_argument("--rate", default="50", help="serve: requests per second (comma list)")
     ap.add_argument("--duration", type=float, default=4.0, help="serve: seconds of arrivals")
     ap.add_argument("--serve-capacity", default=str(1 << 20),
@@ -237,6 +238,9 @@ def make_scene():
         mesh = H.Mesh.generate(2, seed=2)
         nodes, leaf = H.build_kdtree(mesh.points, mesh.triangles)
         return mesh, nodes, leaf, S.terrain_cam(W_RES / H_RES)
+    if SCENE == "room":
+        mesh, nodes, leaf = S.make_scene(0)
+        return mesh, nodes, leaf, S.ROOM_CAM
     mesh, nodes, leaf = S.make_scene(1, seed=1)
     return mesh, nodes, leaf, S.ROOM_CAM
 
@@ -821,7 +825,7 @@ def run_compact(args):
 
 
 def main():
-    global W_RES, H_RES, SPP, WORKLOAD, SCENE, BG
+    global W_RES, H_RES, SPP, DEPTH, WORKLOAD, SCENE, BG
     args = parse()
     if args.mode == "compact":
         run_compact(args)
@@ -840,6 +844,14 @@ def main():
         W_RES, H_RES, SPP = 1920, 1080, 256
         BG = (0.2, 0.2, 0.2)
         WORKLOAD = "terrain_2.4M_tris_1920x1080_spp256_d8"
+    if args.scene == "room":
+        SCENE = "room"
+        W_RES, H_RES, SPP, DEPTH = 256, 256, 16, 5
+        WORKLOAD = "room_38_tris_256x256_spp16_d5"
+    if args.impl == "reference" and SCENE != "spheres":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference arm runs the "
+                          "headline spheres frame only"}))
+        return
     if args.res or args.spp:
         if args.res:
             H_RES = args.res * H_RES // W_RES
