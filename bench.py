@@ -440,6 +440,8 @@ def batch_c3(world, rank):
     import hptracing_b200 as H
     from hptracing_b200 import shard
     from hptracing_b200 import scenes as S
+    import torch
+    dev = torch.cuda.current_device()  # this rank's GPU (set from LOCAL_RANK)
     all_jobs = c3_jobs()
     # With N ranks each runs its share (longest job first onto the least
     # loaded rank); the 32 jobs are the fixed total work (strong scaling).
@@ -452,7 +454,7 @@ def batch_c3(world, rank):
         mesh = H.Mesh.generate(3, seed=j["seed"], family=j["family"], target_triangles=j["tris"])
         nodes, leaf = H.build_kdtree(mesh.points, mesh.triangles)
         cam = S.terrain_cam(1.0) if j["family"] == 2 else S.ROOM_CAM
-        built.append((H.Scene(mesh, nodes, leaf), S.hp_camera(cam),
+        built.append((H.Scene(mesh, nodes, leaf, device=dev), S.hp_camera(cam),
                       H.make_params(j["res"], j["res"], 1, 1, (0.05, 0.05, 0.05), j["spp"],
                                     j["depth"], 0, 1.0, j["seed"]), len(mesh.triangles)))
     build_s = time.perf_counter() - t0
@@ -482,7 +484,7 @@ def batch_c3(world, rank):
         return q, ms, time.perf_counter() - t, accs
 
     def batched():
-        b = H.Batch()
+        b = H.Batch(device=dev)
         b.set_tuning(tune)
         for sc, cam, p, _ in built:
             b.add(sc, cam, p, want_accum=True)
