@@ -1134,8 +1134,11 @@ hpt_tuning default_tuning() {
   // 92.3 / 93.0 ms), 9 blocks of 128 per SM (56 registers; with
   // cooperative tests 8 / 9 / 10 blocks: spheres 94.8 / 92.3 / 101.4 ms,
   // terrain 74.3 / 70.7 / 81.5 ms - at 10 the 48-register budget spills),
-  // no shared-node prefix.
-  t.capacity = 1 << 22;
+  // no shared-node prefix, a wavefront of 2^24 paths (2^22 / 2^23 / 2^24 /
+  // 2^25: spheres 92.2 / 88.7 / 87.0 / 87.1 ms, terrain at 16 spp 227.5 /
+  // 223.0 / 220.3 / 218.4 ms; 3.5 GB of queues, allocated only up to the
+  // paths a run has).
+  t.capacity = 1 << 24;
   t.isect_block = 128;
   t.isect_min_blocks = 9;
   t.shade_block = 256;
@@ -1905,7 +1908,16 @@ hpt_status Engine::run(const std::vector<JobSpec>& jobs, hpt_render_stats* stats
   if (init_status_ != HPT_OK) return fail(init_status_, "engine set-up failed");
   HPT_CUDA(cudaSetDevice(device));
   if (jobs.empty()) return HPT_OK;
-  hpt_status s = ensure_capacity(std::max(1024, tuning.capacity));
+  // The wavefront never holds more paths than the run has, so the queues
+  // are sized to the smaller of the tuning's capacity and the run's paths
+  // (results do not depend on the capacity: fixed-point sums, counter RNG).
+  int64_t paths = 0;
+  for (const JobSpec& js : jobs) {
+    const hpt_render_params& p = js.params;
+    paths += (int64_t)p.sample_x * p.supersample_x * p.sample_y * p.supersample_y * p.sample;
+  }
+  hpt_status s = ensure_capacity(
+      (int)std::max<int64_t>(1024, std::min<int64_t>(tuning.capacity, paths)));
   if (s != HPT_OK) return s;
   s = ensure_slots((int)jobs.size());
   if (s != HPT_OK) return s;

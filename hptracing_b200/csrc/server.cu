@@ -936,7 +936,7 @@ extern "C" hpt_status hpt_autotune(hpt_scene* scene, const hpt_camera* camera,
        [](hpt_tuning& t, int a, int) { t.refill_chunk = a; }},
       {{{0, 0}, {1024, 0}, {2048, 0}, {4096, 0}},
        [](hpt_tuning& t, int a, int) { t.smem_nodes = a; }},
-      {{{1 << 20, 0}, {1 << 21, 0}, {1 << 22, 0}},
+      {{{1 << 20, 0}, {1 << 21, 0}, {1 << 22, 0}, {1 << 23, 0}, {1 << 24, 0}},
        [](hpt_tuning& t, int a, int) { t.capacity = a; }},
       {{{0, 0}, {1, 0}}, [](hpt_tuning& t, int a, int) { t.use_graph = a; }},
       {{{0, 0}, {3, 0}, {4, 0}}, [](hpt_tuning& t, int a, int) { t.shade_min_blocks = a; }},
