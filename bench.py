@@ -940,7 +940,8 @@ def main():
                          "frac": (achieved / peak) if achieved else None,
                          "peak_kind": peak_kind,
                          "traffic": profiled_traffic() if WORKLOAD.startswith("spheres64") else None,
-                         "traffic_source": "ncu --set full, one full-queue launch (profiles/)",
+                         "traffic_source": "ncu dram__bytes_read/write.sum, mean of two full-queue launches "
+                                           "of this frame (profiles/)",
                          "algorithmic_bytes_per_launch": ib / max(1, isect_launches),
                          "launches": isect_launches,
                          "avg_launch_ms": isect_ms / max(1, isect_launches)},
