@@ -272,7 +272,9 @@ hpt_status hpt_render_stats_get(const hpt_scene* scene, hpt_render_stats* out);
 
 /* Engine tuning knobs (defaults come from the autotuner cache when set). */
 typedef struct hpt_tuning {
-  int32_t capacity;          /* paths in flight (wavefront size)          */
+  int32_t capacity;          /* paths in flight (wavefront size); a run's */
+                             /* queues hold at most its rays x spp paths; */
+                             /* default 2^24 (208 B per path)             */
   int32_t isect_block;       /* threads per intersect block (128 / 256)   */
   int32_t shade_block;       /* threads per shade block                   */
   int32_t refill_chunk;      /* lanes idle before a warp refills          */
