@@ -283,6 +283,7 @@ constexpr int kTravStepSmem = 2;  // trav_step with the shared-memory node prefi
 #define HPT_COOP_PRIMARY 0
 #endif
 constexpr bool kCoopPrimary = HPT_COOP_PRIMARY != 0;
+
 // Scene accessors of the traversal loops: scene_of(slot) is the scene of a
 // job slot's rays - the launch's one scene (kernel parameters), the
 // per-block table of a several-scene launch, or the job table.
