@@ -4,6 +4,7 @@ fails loudly (HPT_ERR_CUDA) instead of falling back to the CPU."""
 import ctypes as C
 import os
 import re
+import shutil
 import subprocess
 
 import numpy as np
@@ -179,7 +180,7 @@ _MIRRORS = {
 
 
 def test_ctypes_mirrors_match_the_c_layout(tmp_path):
-    gcc = __import__("shutil").which("gcc")
+    gcc = shutil.which("gcc")
     if not gcc:
         pytest.skip("no C compiler")
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "hpt.h"', 'int main(void) {']
