@@ -538,7 +538,9 @@ HPT_HD bool trav_step(const Sc& s, TravState& st, TravCold& tc, const uint2* sme
   if (st.node < 0) return true;
   const Ray& r = st.ray;
   if (st.phase == kStepDescend) {
-    HPT_DCHECK(err, st.node < s.num_nodes, 101, st.node, { st.node = -1; return true; });
+    // st.node is in range: every value it takes is checked where it is made
+    // (the root, a hint in trav_init, a child at check 106, a rope at check
+    // 105, the root again in trav_finish).
     const uint2 nd = fetch_node(s, smem, kSmem ? n_smem : 0, st.node);
     if ((nd.x >> 30) != kLeafKind) {
       // One descent step; the entry point p = o + t_entry * d on the split
