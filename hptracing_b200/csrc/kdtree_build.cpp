@@ -19,7 +19,7 @@
 //    filtered arrays hold the same values in the same order; the one case
 //    where the order of equal values shows in the output (+0.0 and -0.0 in
 //    one candidate list, see best_split) recomputes that axis the
-//    reference's way, and so do small nodes (thread-local scratch);
+//    reference's way. Small nodes keep their arrays on a per-thread stack;
 //  - the candidate list is a merge of the two sorted arrays instead of a
 //    re-sort;
 //  - nodes come from per-thread arenas, subtrees are built by a pool of
@@ -79,14 +79,72 @@ struct NodeLists {
   std::vector<Keyed> mins[3], maxs[3];
 };
 
+// A node's sorted arrays wherever they live: n entries per axis and side,
+// in a node's own vectors (large nodes) or in its thread's list stack.
+struct ListView {
+  const Keyed* mins[3];
+  const Keyed* maxs[3];
+  size_t n;
+};
+
+ListView view_of(const NodeLists& L) {
+  ListView v;
+  for (int d = 0; d < 3; ++d) {
+    v.mins[d] = L.mins[d].data();
+    v.maxs[d] = L.maxs[d].data();
+  }
+  v.n = L.mins[0].size();
+  return v;
+}
+
+// Per-thread stack of the small nodes' arrays: a node's children take their
+// arrays from it and give them back once both subtrees are built, so the
+// arrays of a depth-first build live in a few reused chunks instead of
+// being allocated per node. Chunks never move, so pointers stay valid.
+struct ListStack {
+  static constexpr size_t kChunk = size_t(1) << 20;  // Keyed entries
+  std::vector<std::unique_ptr<Keyed[]>> chunks;
+  std::vector<size_t> caps;
+  size_t chunk = 0, used = 0;
+  struct Mark {
+    size_t chunk, used;
+  };
+  Mark mark() const { return {chunk, used}; }
+  void release(Mark m) {
+    chunk = m.chunk;
+    used = m.used;
+  }
+  Keyed* alloc(size_t n) {
+    if (chunks.empty()) {
+      chunks.emplace_back(new Keyed[std::max(n, kChunk)]);
+      caps.push_back(std::max(n, kChunk));
+    } else if (used + n > caps[chunk]) {
+      // The chunks past the current one are free (last in, first out).
+      ++chunk;
+      used = 0;
+      if (chunk == chunks.size()) {
+        chunks.emplace_back(new Keyed[std::max(n, kChunk)]);
+        caps.push_back(std::max(n, kChunk));
+      } else if (caps[chunk] < n) {
+        chunks[chunk].reset(new Keyed[n]);
+        caps[chunk] = n;
+      }
+    }
+    Keyed* p = chunks[chunk].get() + used;
+    used += n;
+    return p;
+  }
+};
+
 // A child subtree of more than this many triangles is handed to the worker
 // pool when a worker is idle; smaller ones are built by the thread that
 // split their parent.
 constexpr size_t kTaskMin = 1024;
 // Nodes above this many triangles scan their three axes on three threads.
 constexpr size_t kParallelAxes = 1 << 15;
-// Nodes up to this many triangles sort their own values (in thread-local
-// scratch) instead of receiving filtered arrays from their parent.
+// Nodes up to this many triangles keep their filtered arrays on their
+// thread's list stack; larger ones own vectors (they may move to another
+// thread with their subtree).
 constexpr size_t kSmallNode = 256;
 
 std::atomic<uint64_t> g_builder_generation{0};
@@ -201,31 +259,31 @@ struct Builder {
     std::sort(mx.begin(), mx.end(), by_value);
   }
 
-  static bool mixed_zeros(const std::vector<Keyed>& a, const std::vector<Keyed>& b) {
+  static bool mixed_zeros(const Keyed* a, const Keyed* b, size_t n) {
     bool pos_zero = false, neg_zero = false;
-    for (const std::vector<Keyed>* v : {&a, &b})
-      for (const Keyed& k : *v)
-        if (k.v == 0.f) (std::signbit(k.v) ? neg_zero : pos_zero) = true;
+    for (const Keyed* v : {a, b})
+      for (size_t i = 0; i < n; ++i)
+        if (v[i].v == 0.f) (std::signbit(v[i].v) ? neg_zero : pos_zero) = true;
     return pos_zero && neg_zero;
   }
 
   // Best split along axis d (kdtree.cpp:47-89), from the node's filtered
   // arrays when it has them (L != nullptr), else from its own sort.
-  void axis_split(const Node* node, const NodeLists* L, int d, float& best_pos,
+  void axis_split(const Node* node, const ListView* L, int d, float& best_pos,
                   float& best_cost) const {
     thread_local std::vector<float> mins, maxs;
-    if (!L || mixed_zeros(L->mins[d], L->maxs[d])) {
+    if (!L || mixed_zeros(L->mins[d], L->maxs[d], L->n)) {
       // The order of +0.0 and -0.0 among themselves is the reference's sort
       // order of this node's own arrays: small nodes, and this rare case,
       // compute them its way.
       min_max(node->geo, d, mins, maxs);
     } else {
-      const std::vector<Keyed>& mn = L->mins[d];
-      const std::vector<Keyed>& mx = L->maxs[d];
-      mins.resize(mn.size());
-      maxs.resize(mx.size());
-      for (size_t i = 0; i < mn.size(); ++i) mins[i] = mn[i].v;
-      for (size_t i = 0; i < mx.size(); ++i) maxs[i] = mx[i].v;
+      const Keyed* mn = L->mins[d];
+      const Keyed* mx = L->maxs[d];
+      mins.resize(L->n);
+      maxs.resize(L->n);
+      for (size_t i = 0; i < L->n; ++i) mins[i] = mn[i].v;
+      for (size_t i = 0; i < L->n; ++i) maxs[i] = mx[i].v;
     }
     best_split(mins, maxs, node->box_start[d], node->box_end[d], best_pos, best_cost);
   }
@@ -271,12 +329,13 @@ struct Builder {
     }
   }
 
-  // kdtree.cpp:93-169. L: the node's filtered sorted arrays (consumed), or
-  // empty for a node of at most kSmallNode triangles.
-  void split(Node* node, NodeLists L) {
+  // kdtree.cpp:93-169. The node's filtered sorted arrays: `small` (on this
+  // thread's list stack) when given, else L (consumed).
+  void split(Node* node, NodeLists L, const ListView* small = nullptr) {
     const size_t n = node->geo.size();
     if (n < 5) return;
-    const NodeLists* lists = n > kSmallNode ? &L : nullptr;
+    const ListView own = small ? *small : view_of(L);
+    const ListView* lists = &own;
     float no_split_cost = 3.f * n;
     float best_pos[3], best_val[3];
     if (n > kParallelAxes) {
@@ -328,29 +387,44 @@ struct Builder {
       }
     }
     std::vector<int32_t>().swap(node->geo);
-    // The children's sorted arrays: the node's, filtered (order kept).
+    // The children's sorted arrays: the node's, filtered (order kept) - a
+    // large child's into its own vectors, a small child's onto this
+    // thread's list stack, given back once both subtrees are built (small
+    // subtrees are always built here, depth first).
+    thread_local ListStack stack;
+    const ListStack::Mark mark = stack.mark();
+    const bool big_l = nl > kSmallNode, big_r = nr > kSmallNode;
     NodeLists LL, RL;
-    if (lists) {
-      const bool need_l = nl > kSmallNode, need_r = nr > kSmallNode;
-      for (int d = 0; d < 3; ++d) {
-        for (int m = 0; m < 2; ++m) {
-          std::vector<Keyed>& src = m ? L.maxs[d] : L.mins[d];
-          std::vector<Keyed>& dl = m ? LL.maxs[d] : LL.mins[d];
-          std::vector<Keyed>& dr = m ? RL.maxs[d] : RL.mins[d];
-          if (need_l) dl.reserve(nl);
-          if (need_r) dr.reserve(nr);
-          for (const Keyed& k : src) {
-            const uint8_t sd = side[k.id];
-            if (need_l && (sd & 1)) dl.push_back(k);
-            if (need_r && (sd & 2)) dr.push_back(k);
-          }
-          std::vector<Keyed>().swap(src);
+    ListView SL{}, SR{};
+    SL.n = nl;
+    SR.n = nr;
+    for (int d = 0; d < 3; ++d) {
+      for (int m = 0; m < 2; ++m) {
+        const Keyed* src = m ? lists->maxs[d] : lists->mins[d];
+        std::vector<Keyed>& vl = m ? LL.maxs[d] : LL.mins[d];
+        std::vector<Keyed>& vr = m ? RL.maxs[d] : RL.mins[d];
+        if (big_l) vl.resize(nl);
+        if (big_r) vr.resize(nr);
+        Keyed* dl = big_l ? vl.data() : stack.alloc(nl);
+        Keyed* dr = big_r ? vr.data() : stack.alloc(nr);
+        (m ? SL.maxs[d] : SL.mins[d]) = dl;
+        (m ? SR.maxs[d] : SR.mins[d]) = dr;
+        size_t il = 0, ir = 0;
+        for (size_t i = 0; i < n; ++i) {
+          const Keyed k = src[i];
+          const uint8_t sd = side[k.id];
+          if (sd & 1) dl[il++] = k;
+          if (sd & 2) dr[ir++] = k;
         }
       }
     }
+    if (!small) L = NodeLists();  // the node's own vectors are spent
     // The two subtrees are independent.
-    build_subtree(r, std::move(RL));
-    build_subtree(l, std::move(LL));
+    if (big_r) build_subtree(r, std::move(RL));
+    else split(r, NodeLists(), &SR);
+    if (big_l) build_subtree(l, std::move(LL));
+    else split(l, NodeLists(), &SL);
+    stack.release(mark);
   }
 
   // kdtree.cpp:171-206
@@ -444,7 +518,6 @@ hpt_status build_kdtree(const F4* points, int num_points, const I4* tris,
     root->box_start[d] = lists.mins[d].front().v - 1e-3f;
     root->box_end[d] = lists.maxs[d].back().v + 1e-3f;
   }
-  if ((size_t)num_tris <= kSmallNode) lists = NodeLists();
   b.run(root, std::move(lists), num_threads);
   Builder::remove_empty(root);
 
