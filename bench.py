@@ -285,24 +285,26 @@ def isect_bytes(stats):
             48 * stats["triangle_tests"])
 
 
-def cpu_baseline(mesh, nodes, leaf, cam, kind):
+def cpu_baseline(mesh, nodes, leaf, cam, kind, samples=1):
     """The reference's kernels (kind 'reference') or the oracle restatement
-    ('port') on all host cores, bounded sample: 1 sample of the frame."""
+    ('port') on all host cores, bounded sample: `samples` samples per ray of
+    the frame."""
     import oracle as O
     cs = O.CpuScene(mesh, nodes, leaf)
     threads = os.cpu_count() or 1
     t0 = time.perf_counter()
     if kind == "reference":
-        _, _, counts = cs.refcl_render(cam, W_RES, H_RES, 1, 1, BG, 1, DEPTH, 0, 1.0,
+        _, _, counts = cs.refcl_render(cam, W_RES, H_RES, 1, 1, BG, samples, DEPTH, 0, 1.0,
                                        seed=1, threads=threads)
     else:
-        _, _, counts = cs.render(cam, W_RES, H_RES, 1, 1, BG, 1, DEPTH, 0, seed=1,
+        _, _, counts = cs.render(cam, W_RES, H_RES, 1, 1, BG, samples, DEPTH, 0, seed=1,
                                  rng_mode=0, threads=threads)
     dt = time.perf_counter() - t0
     return {"value": counts[0] / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": kind,
             "seconds": dt,
-            "sample": "%dx%d rays x 1 sample x depth %d of the same frame (%d queries, %.1f s)"
-                      % (W_RES, H_RES, DEPTH, int(counts[0]), dt)}
+            "sample": "%dx%d rays x %d sample%s x depth %d of the same frame (%d queries, %.1f s)"
+                      % (W_RES, H_RES, samples, "" if samples == 1 else "s", DEPTH,
+                         int(counts[0]), dt)}
 
 
 def run_reference(args):
@@ -925,6 +927,11 @@ def main():
         obuild.build()
         kind = "reference" if O.refcl_lib() is not None else "port"
         base = cpu_baseline(mesh, nodes, leaf, cam, kind)
+        # About 10 s of CPU work: as many samples per ray (up to the frame's)
+        # as one sample's time allows.
+        samples = max(1, min(SPP, int(10.0 / max(base["seconds"], 1e-3))))
+        if samples > 1:
+            base = cpu_baseline(mesh, nodes, leaf, cam, kind, samples)
     line = None
     if rank == 0:
         line = {
