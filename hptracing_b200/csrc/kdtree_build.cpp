@@ -398,25 +398,43 @@ struct Builder {
     ListView SL{}, SR{};
     SL.n = nl;
     SR.n = nr;
+    const uint8_t* sides = side.data();
+    auto filter = [&](const Keyed* src, Keyed* dl, Keyed* dr) {
+      size_t il = 0, ir = 0;
+      for (size_t i = 0; i < n; ++i) {
+        const Keyed k = src[i];
+        const uint8_t sd = sides[k.id];
+        if (sd & 1) dl[il++] = k;
+        if (sd & 2) dr[ir++] = k;
+      }
+    };
+    Keyed* dst[3][2][2];  // [axis][min/max][left/right]
     for (int d = 0; d < 3; ++d) {
       for (int m = 0; m < 2; ++m) {
-        const Keyed* src = m ? lists->maxs[d] : lists->mins[d];
         std::vector<Keyed>& vl = m ? LL.maxs[d] : LL.mins[d];
         std::vector<Keyed>& vr = m ? RL.maxs[d] : RL.mins[d];
         if (big_l) vl.resize(nl);
         if (big_r) vr.resize(nr);
-        Keyed* dl = big_l ? vl.data() : stack.alloc(nl);
-        Keyed* dr = big_r ? vr.data() : stack.alloc(nr);
-        (m ? SL.maxs[d] : SL.mins[d]) = dl;
-        (m ? SR.maxs[d] : SR.mins[d]) = dr;
-        size_t il = 0, ir = 0;
-        for (size_t i = 0; i < n; ++i) {
-          const Keyed k = src[i];
-          const uint8_t sd = side[k.id];
-          if (sd & 1) dl[il++] = k;
-          if (sd & 2) dr[ir++] = k;
-        }
+        dst[d][m][0] = big_l ? vl.data() : stack.alloc(nl);
+        dst[d][m][1] = big_r ? vr.data() : stack.alloc(nr);
+        (m ? SL.maxs[d] : SL.mins[d]) = dst[d][m][0];
+        (m ? SR.maxs[d] : SR.mins[d]) = dst[d][m][1];
       }
+    }
+    auto filter_axis = [&](int d) {
+      filter(lists->mins[d], dst[d][0][0], dst[d][0][1]);
+      filter(lists->maxs[d], dst[d][1][0], dst[d][1][1]);
+    };
+    if (n > kParallelAxes) {
+      // The six arrays of a large node are independent: one axis per thread
+      // (the side table is only read here).
+      std::thread t1([&] { filter_axis(1); });
+      std::thread t2([&] { filter_axis(2); });
+      filter_axis(0);
+      t1.join();
+      t2.join();
+    } else {
+      for (int d = 0; d < 3; ++d) filter_axis(d);
     }
     if (!small) L = NodeLists();  // the node's own vectors are spent
     // The two subtrees are independent.
